@@ -1,0 +1,222 @@
+"""ctypes binding of libinching_b200.so (the C ABI declared in include/inching_b200.h).
+
+There is no fallback: if the shared library is missing or CUDA is unavailable the
+calls raise.  Device buffers are torch CUDA tensors passed by data pointer, on
+torch's current stream; workspaces come from torch's caching allocator.
+"""
+from __future__ import annotations
+
+import ctypes
+import os
+from ctypes import POINTER, Structure, c_double, c_int32, c_int64, c_size_t, c_void_p, c_char_p
+
+import torch
+
+HERE = os.path.dirname(os.path.abspath(__file__))
+LIB_PATH = os.path.join(HERE, "libinching_b200.so")
+
+INCH_OK, INCH_INVALID_ARG, INCH_OOM, INCH_NOT_CONVERGED, INCH_TIMEOUT, INCH_CUDA_ERROR, INCH_LIMIT = range(7)
+MAX_DEGREE = 1024
+
+
+class InchError(RuntimeError):
+    def __init__(self, status, msg):
+        super().__init__(f"inching_b200 error {status}: {msg}")
+        self.status = status
+
+
+class CellGrid(Structure):
+    _fields_ = [("origin", c_double * 3), ("cell", c_double), ("dims", c_int32 * 3),
+                ("ncells", c_int64), ("n_atoms", c_int64)]
+
+
+class SpmmEpilogue(Structure):
+    _fields_ = [("alpha", c_double), ("gamma", c_double), ("beta", c_double), ("mu", c_double),
+                ("hot_shift", c_double), ("r", c_int32), ("accumulate", c_int32)]
+
+
+_lib = None
+
+# name -> (restype, argtypes)
+_SIGS = {
+    "inch_last_error_string": (c_char_p, []),
+    "inch_abi_version": (ctypes.c_int, []),
+    "inch_cell_grid_plan": (ctypes.c_int, [c_void_p, c_int64, c_double, POINTER(CellGrid), c_void_p, c_size_t, c_void_p]),
+    "inch_neighbors_workspace_size": (c_size_t, [POINTER(CellGrid)]),
+    "inch_neighbors_count": (ctypes.c_int, [c_void_p, POINTER(CellGrid), c_double, c_void_p, c_void_p,
+                                            POINTER(c_int64), c_void_p, c_size_t, c_void_p]),
+    "inch_neighbors_fill": (ctypes.c_int, [c_void_p, POINTER(CellGrid), c_double, c_void_p, c_void_p,
+                                           c_void_p, c_size_t, c_void_p]),
+    "inch_rcm_workspace_size": (c_size_t, [c_int64]),
+    "inch_rcm": (ctypes.c_int, [c_void_p, c_void_p, c_void_p, c_void_p, c_int64, c_void_p, c_void_p,
+                                POINTER(c_int32), c_void_p, c_size_t, c_void_p]),
+    "inch_band_slices_workspace_size": (c_size_t, [c_int64, c_int64]),
+    "inch_band_slices": (ctypes.c_int, [c_void_p, c_void_p, c_int64, c_void_p, c_int64, c_int64, c_int32,
+                                        c_void_p, c_void_p, c_void_p, POINTER(c_int64), c_void_p, c_size_t,
+                                        c_void_p]),
+    "inch_hessian_assemble": (ctypes.c_int, [c_void_p, c_int64, c_double, c_double, c_void_p, c_void_p,
+                                             c_void_p, c_void_p, c_void_p, c_void_p, c_void_p]),
+    "inch_spmm_workspace_size": (c_size_t, [c_int64, c_int32, c_int32]),
+    "inch_spmm": (ctypes.c_int, [c_int32, c_int64, c_void_p, c_void_p, c_void_p, c_void_p, c_int64, c_int32,
+                                 c_void_p, c_int64, c_void_p, c_int64, c_void_p, c_int64, c_void_p,
+                                 POINTER(SpmmEpilogue), c_void_p, c_size_t, c_void_p]),
+}
+
+
+def exported_symbols():
+    """Names of the C-ABI entry points this binding declares."""
+    return sorted(_SIGS)
+
+
+def lib():
+    """Load the shared library once; raise if it is missing (no CPU fallback)."""
+    global _lib
+    if _lib is not None:
+        return _lib
+    if not os.path.exists(LIB_PATH):
+        raise ImportError(f"{LIB_PATH} is missing: build it with `python -m inching_b200.build` "
+                          "(the CUDA path has no fallback)")
+    L = ctypes.CDLL(LIB_PATH)
+    for name, (res, args) in _SIGS.items():
+        f = getattr(L, name)
+        f.restype = res
+        f.argtypes = args
+    _lib = L
+    return L
+
+
+def check(status: int):
+    if status == INCH_OK:
+        return
+    msg = lib().inch_last_error_string().decode(errors="replace")
+    if status == INCH_INVALID_ARG:
+        raise AssertionError(msg if msg.startswith("ABORTED") else "ABORTED. " + msg)
+    raise InchError(status, msg)
+
+
+def _ptr(t):
+    return ctypes.c_void_p(t.data_ptr()) if t is not None else ctypes.c_void_p(0)
+
+
+def _stream():
+    return ctypes.c_void_p(torch.cuda.current_stream().cuda_stream)
+
+
+def _ws(nbytes, device):
+    return torch.empty(max(int(nbytes), 256), dtype=torch.uint8, device=device)
+
+
+def _require_cuda(t, name, dtype=None):
+    if not (isinstance(t, torch.Tensor) and t.is_cuda):
+        raise AssertionError(f"ABORTED. {name} must be a CUDA tensor")
+    if dtype is not None and t.dtype != dtype:
+        raise AssertionError(f"ABORTED. {name} must be {dtype}, got {t.dtype}")
+    if not t.is_contiguous():
+        raise AssertionError(f"ABORTED. {name} must be contiguous")
+
+
+# ---------------------------------------------------------------------------
+# Neighbours, Cuthill-McKee, band slices
+# ---------------------------------------------------------------------------
+def neighbor_lists(X: torch.Tensor, rc_nm: float):
+    """(degree int32 (N,), rowptr int64 (N+1,), cols int32 (nnz,)) on X's device."""
+    _require_cuda(X, "X", torch.float64)
+    L = lib()
+    n = X.shape[0]
+    dev = X.device
+    grid = CellGrid()
+    w0 = _ws(256, dev)
+    check(L.inch_cell_grid_plan(_ptr(X), n, rc_nm, ctypes.byref(grid), _ptr(w0), w0.numel(), _stream()))
+    ws = _ws(L.inch_neighbors_workspace_size(ctypes.byref(grid)), dev)
+    degree = torch.empty(n, dtype=torch.int32, device=dev)
+    rowptr = torch.empty(n + 1, dtype=torch.int64, device=dev)
+    nnz = c_int64(0)
+    check(L.inch_neighbors_count(_ptr(X), ctypes.byref(grid), rc_nm, _ptr(degree), _ptr(rowptr),
+                                 ctypes.byref(nnz), _ptr(ws), ws.numel(), _stream()))
+    cols = torch.empty(max(nnz.value, 1), dtype=torch.int32, device=dev)[:nnz.value]
+    check(L.inch_neighbors_fill(_ptr(X), ctypes.byref(grid), rc_nm, _ptr(rowptr), _ptr(cols),
+                                _ptr(ws), ws.numel(), _stream()))
+    return degree, rowptr, cols
+
+
+def cuthill_mckee(rowptr, cols, degree, seed_order):
+    """Reversed Cuthill-McKee order and its inverse (int64 device tensors), levels."""
+    for t, nm, dt in ((rowptr, "rowptr", torch.int64), (cols, "cols", torch.int32),
+                      (degree, "degree", torch.int32), (seed_order, "seed_order", torch.int64)):
+        _require_cuda(t, nm, dt)
+    L = lib()
+    n = degree.shape[0]
+    dev = degree.device
+    ws = _ws(L.inch_rcm_workspace_size(n), dev)
+    order = torch.empty(n, dtype=torch.int64, device=dev)
+    undo = torch.empty(n, dtype=torch.int64, device=dev)
+    levels = c_int32(0)
+    check(L.inch_rcm(_ptr(rowptr), _ptr(cols), _ptr(degree), _ptr(seed_order), n, _ptr(order), _ptr(undo),
+                     ctypes.byref(levels), _ptr(ws), ws.numel(), _stream()))
+    return order, undo, levels.value
+
+
+def band_slices(rowptr, cols, n_atoms, heads, gap=100, max_slices=256):
+    """Per-batch (counts int32, starts int64 (nb, max_slices), ends, total neighbours)."""
+    _require_cuda(rowptr, "rowptr", torch.int64)
+    _require_cuda(cols, "cols", torch.int32)
+    _require_cuda(heads, "heads", torch.int64)
+    L = lib()
+    nb = heads.shape[0] - 1
+    dev = rowptr.device
+    nnz = int(rowptr[n_atoms].item())
+    ws = _ws(L.inch_band_slices_workspace_size(nb, nnz), dev)
+    starts = torch.empty((nb, max_slices), dtype=torch.int64, device=dev)
+    ends = torch.empty((nb, max_slices), dtype=torch.int64, device=dev)
+    counts = torch.empty(nb, dtype=torch.int32, device=dev)
+    total = c_int64(0)
+    check(L.inch_band_slices(_ptr(rowptr), _ptr(cols), n_atoms, _ptr(heads), nb, gap, max_slices, _ptr(starts),
+                             _ptr(ends), _ptr(counts), ctypes.byref(total), _ptr(ws), ws.numel(), _stream()))
+    return counts, starts, ends, total.value
+
+
+# ---------------------------------------------------------------------------
+# Hessian store and operator
+# ---------------------------------------------------------------------------
+def hessian_assemble(X, rowptr, cols, rc_nm, plus_i, want64=True, want32=True):
+    _require_cuda(X, "X", torch.float64)
+    _require_cuda(rowptr, "rowptr", torch.int64)
+    _require_cuda(cols, "cols", torch.int32)
+    n = X.shape[0]
+    nnz = cols.shape[0]
+    dev = X.device
+    ent64 = torch.empty((nnz, 4), dtype=torch.float64, device=dev) if want64 else None
+    diag64 = torch.empty((n, 8), dtype=torch.float64, device=dev) if want64 else None
+    ent32 = torch.empty((nnz, 4), dtype=torch.float32, device=dev) if want32 else None
+    diag32 = torch.empty((n, 8), dtype=torch.float32, device=dev) if want32 else None
+    check(lib().inch_hessian_assemble(_ptr(X), n, rc_nm, plus_i, _ptr(rowptr), _ptr(cols), _ptr(ent64),
+                                      _ptr(diag64), _ptr(ent32), _ptr(diag32), _stream()))
+    return ent64, diag64, ent32, diag32
+
+
+_ws_cache = {}
+
+
+def spmm(prec, n_atoms, rowptr, ent, diag, X, Y, *, alpha=1.0, gamma=0.0, beta=0.0, Yin=None,
+         acc=None, mu=0.0, Q=None, hot_shift=0.0):
+    """Y = alpha*(H X) + gamma*X + beta*Yin + hot_shift*Q^T(Q X); acc += mu*Y if acc given.
+
+    X, Y, Yin, acc: (3N,) or (3N, b) tensors whose last dimension is contiguous."""
+    L = lib()
+    b = 1 if X.dim() == 1 else X.shape[1]
+    ldx = 1 if X.dim() == 1 else X.stride(0)
+    ldy = 1 if Y.dim() == 1 else Y.stride(0)
+    ldyin = 0 if Yin is None else (1 if Yin.dim() == 1 else Yin.stride(0))
+    ldacc = 0 if acc is None else (1 if acc.dim() == 1 else acc.stride(0))
+    r = 0 if Q is None else Q.shape[0]
+    ep = SpmmEpilogue(alpha, gamma, beta, mu, hot_shift, r, 1 if acc is not None else 0)
+    dev = X.device
+    key = (dev.index, r > 0)
+    ws = _ws_cache.get(key)
+    if ws is None:
+        ws = _ws(L.inch_spmm_workspace_size(n_atoms, b, r), dev)
+        _ws_cache[key] = ws
+    check(L.inch_spmm(prec, n_atoms, _ptr(rowptr), _ptr(ent), _ptr(diag), _ptr(X), ldx, b, _ptr(Y), ldy,
+                      _ptr(Yin), ldyin, _ptr(acc), ldacc, _ptr(Q), ctypes.byref(ep), _ptr(ws), ws.numel(),
+                      _stream()))
+    return Y

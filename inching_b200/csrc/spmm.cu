@@ -1,0 +1,255 @@
+// Hessian x multivector on the rank-one block store, with a fused epilogue.
+//
+// Reference operator: InchingLiteInteger/Burn/Krylov/T3.py:54-165 computes
+// u = L v + L^T v - diag(A) v with two cuSPARSE CSR SpMVs over the scalar lower
+// triangle, one vector at a time.  Here one pass streams the full (both
+// triangles) rank-one store once per multivector tile:
+//     (H X)_i = D_i X_i - sum_j w_ij (w_ij . X_j)
+// and applies, per output element, the epilogue
+//     Y = alpha*(H X) + gamma*X + beta*Yin + hot_shift * Q^T (Q X)   [Acc += mu*Y]
+// which covers the shift of the JD correction operator (JacobiDavidson.../T1.py:
+// 67-331), explicit Hotelling deflation (Orthogonalization/T3.py:62-164) and one
+// three-term Chebyshev step with its accumulation (PolynomialFilters/T2.py:59-80).
+//
+// Thread mapping: a group of G lanes owns one atom row (3 dofs x B columns); the
+// lanes of the group stride over the row's entries (one 16-byte load per entry in
+// FP32, two in FP64), gather X_j from L1/L2 (rows are banded after Cuthill-McKee
+// so neighbouring rows share their X_j), and reduce with xor shuffles.
+#include "common.cuh"
+
+namespace inch {
+namespace {
+
+struct Epi {
+  double alpha, gamma, beta, mu;
+  int r, accumulate, has_yin;
+};
+
+template <class T>
+struct Ent;
+template <>
+struct Ent<float> {
+  __device__ __forceinline__ static void load(const void* base, int64_t e, float& wx, float& wy, float& wz, int& j) {
+    float4 v = __ldg(reinterpret_cast<const float4*>(base) + e);
+    wx = v.x;
+    wy = v.y;
+    wz = v.z;
+    j = __float_as_int(v.w);
+  }
+};
+template <>
+struct Ent<double> {
+  __device__ __forceinline__ static void load(const void* base, int64_t e, double& wx, double& wy, double& wz,
+                                              int& j) {
+    const double2* p = reinterpret_cast<const double2*>(base) + 2 * e;
+    double2 a = __ldg(p), b = __ldg(p + 1);
+    wx = a.x;
+    wy = a.y;
+    wz = b.x;
+    j = static_cast<int>(b.y);
+  }
+};
+
+constexpr int kThreads = 256;
+
+template <class T, int B, int G>
+__global__ void __launch_bounds__(kThreads)
+k_spmm(int64_t n_atoms, const int64_t* __restrict__ rowptr, const void* __restrict__ ent,
+       const T* __restrict__ diag, const T* __restrict__ X, int64_t ldx, T* Y, int64_t ldy, const T* Yin,
+       int64_t ldyin, T* __restrict__ Acc, int64_t ldacc, int c0, Epi ep, const double* __restrict__ Q,
+       int64_t ndof, const double* __restrict__ coef) {
+  __shared__ double s_coef[8 * B];
+  if (ep.r > 0) {
+    for (int t = threadIdx.x; t < ep.r * B; t += kThreads) s_coef[t] = coef[t];
+    __syncthreads();
+  }
+  const int lg = threadIdx.x % G;
+  const int64_t groups = (int64_t)gridDim.x * (kThreads / G);
+  for (int64_t i = (int64_t)blockIdx.x * (kThreads / G) + threadIdx.x / G; i < n_atoms; i += groups) {
+    T acc[3][B];
+#pragma unroll
+    for (int c = 0; c < B; ++c) acc[0][c] = acc[1][c] = acc[2][c] = T(0);
+    const int64_t e1 = rowptr[i + 1];
+    for (int64_t e = rowptr[i] + lg; e < e1; e += G) {
+      T wx, wy, wz;
+      int j;
+      Ent<T>::load(ent, e, wx, wy, wz, j);
+      const T* xj = X + 3 * (int64_t)j * ldx + c0;
+#pragma unroll
+      for (int c = 0; c < B; ++c) {
+        T dot = wx * __ldg(xj + c) + wy * __ldg(xj + ldx + c) + wz * __ldg(xj + 2 * ldx + c);
+        acc[0][c] -= wx * dot;
+        acc[1][c] -= wy * dot;
+        acc[2][c] -= wz * dot;
+      }
+    }
+#pragma unroll
+    for (int o = G / 2; o > 0; o >>= 1) {
+#pragma unroll
+      for (int c = 0; c < B; ++c) {
+        acc[0][c] += __shfl_xor_sync(0xffffffffu, acc[0][c], o);
+        acc[1][c] += __shfl_xor_sync(0xffffffffu, acc[1][c], o);
+        acc[2][c] += __shfl_xor_sync(0xffffffffu, acc[2][c], o);
+      }
+    }
+    const T* d = diag + 8 * i;
+    const T dxx = d[0], dyy = d[1], dzz = d[2], dxy = d[3], dxz = d[4], dyz = d[5];
+#pragma unroll
+    for (int c = 0; c < B; ++c) {
+      if ((c % G) != lg) continue;
+      const int64_t r0 = 3 * i;
+      const T x0 = X[r0 * ldx + c0 + c], x1 = X[(r0 + 1) * ldx + c0 + c], x2 = X[(r0 + 2) * ldx + c0 + c];
+      T h[3];
+      h[0] = acc[0][c] + dxx * x0 + dxy * x1 + dxz * x2;
+      h[1] = acc[1][c] + dxy * x0 + dyy * x1 + dyz * x2;
+      h[2] = acc[2][c] + dxz * x0 + dyz * x1 + dzz * x2;
+      const T xs[3] = {x0, x1, x2};
+#pragma unroll
+      for (int a = 0; a < 3; ++a) {
+        const int64_t row = r0 + a;
+        double y = ep.alpha * (double)h[a] + ep.gamma * (double)xs[a];
+        if (ep.has_yin) y += ep.beta * (double)Yin[row * ldyin + c0 + c];
+        for (int q = 0; q < ep.r; ++q) y += Q[q * ndof + row] * s_coef[q * B + c];
+        Y[row * ldy + c0 + c] = (T)y;
+        if (ep.accumulate) Acc[row * ldacc + c0 + c] += (T)(ep.mu * y);
+      }
+    }
+  }
+}
+
+// Partial sums of Q X over a dof range (blockIdx.x), one deflation vector per
+// blockIdx.y; thread t accumulates column t % B.
+template <class T, int B>
+__global__ void __launch_bounds__(kThreads)
+k_qx_partial(const double* __restrict__ Q, int64_t ndof, const T* __restrict__ X, int64_t ldx, int c0,
+             double* __restrict__ partial) {
+  __shared__ double s[kThreads / 32][32];
+  const int q = blockIdx.y, r = gridDim.y;
+  const double* qr = Q + q * ndof;
+  const int c = threadIdx.x % B;
+  double acc = 0.0;
+  const int64_t total = ndof * B;
+  for (int64_t p = (int64_t)blockIdx.x * kThreads + threadIdx.x; p < total; p += (int64_t)gridDim.x * kThreads) {
+    const int64_t dof = p / B;
+    acc += qr[dof] * (double)X[dof * ldx + c0 + c];
+  }
+#pragma unroll
+  for (int o = 16; o >= B; o >>= 1) acc += __shfl_xor_sync(0xffffffffu, acc, o);
+  const int lane = threadIdx.x & 31, w = threadIdx.x >> 5;
+  if (lane < B) s[w][lane] = acc;
+  __syncthreads();
+  if (threadIdx.x < B) {
+    double t = 0.0;
+    for (int k = 0; k < kThreads / 32; ++k) t += s[k][threadIdx.x];
+    partial[((int64_t)blockIdx.x * r + q) * B + threadIdx.x] = t;
+  }
+}
+
+__global__ void k_qx_final(const double* __restrict__ partial, int P, int r, int B, double shift,
+                           double* __restrict__ coef) {
+  const int t = threadIdx.x;
+  if (t < r * B) {
+    double s = 0.0;
+    for (int p = 0; p < P; ++p) s += partial[(int64_t)p * r * B + t];
+    coef[t] = shift * s;
+  }
+}
+
+constexpr int kQxBlocks = 296;
+
+template <class T, int B, int G>
+cudaError_t launch_tile(int64_t n_atoms, const int64_t* rowptr, const void* ent, const T* diag, const T* X,
+                        int64_t ldx, T* Y, int64_t ldy, const T* Yin, int64_t ldyin, T* Acc, int64_t ldacc, int c0,
+                        Epi ep, const double* Q, double hot_shift, double* partial, double* coef,
+                        cudaStream_t stream) {
+  const int64_t ndof = 3 * n_atoms;
+  if (ep.r > 0) {
+    dim3 g(kQxBlocks, ep.r);
+    k_qx_partial<T, B><<<g, kThreads, 0, stream>>>(Q, ndof, X, ldx, c0, partial);
+    k_qx_final<<<1, 256, 0, stream>>>(partial, kQxBlocks, ep.r, B, hot_shift, coef);
+  }
+  const int rows_per_block = kThreads / G;
+  const int blocks = grid_for(n_atoms, rows_per_block, 148 * 16);
+  k_spmm<T, B, G><<<blocks, kThreads, 0, stream>>>(n_atoms, rowptr, ent, diag, X, ldx, Y, ldy, Yin, ldyin, Acc,
+                                                   ldacc, c0, ep, Q, ndof, coef);
+  return cudaGetLastError();
+}
+
+template <class T>
+cudaError_t run(int64_t n_atoms, const int64_t* rowptr, const void* ent, const void* diag, const void* Xv,
+                int64_t ldx, int b, void* Yv, int64_t ldy, const void* Yinv, int64_t ldyin, void* Accv, int64_t ldacc,
+                Epi ep, const double* Q, double hot_shift, double* partial, double* coef, cudaStream_t s) {
+  const T* X = static_cast<const T*>(Xv);
+  T* Y = static_cast<T*>(Yv);
+  const T* Yin = static_cast<const T*>(Yinv);
+  T* Acc = static_cast<T*>(Accv);
+  const T* D = static_cast<const T*>(diag);
+  int c0 = 0;
+  cudaError_t e = cudaSuccess;
+  while (c0 < b && e == cudaSuccess) {
+    const int rem = b - c0;
+#define TILE(BB, GG)                                                                                          \
+  e = launch_tile<T, BB, GG>(n_atoms, rowptr, ent, D, X, ldx, Y, ldy, Yin, ldyin, Acc, ldacc, c0, ep, Q,     \
+                             hot_shift, partial, coef, s);                                                     \
+  c0 += BB;
+    if (rem >= 16 && sizeof(T) == 4) { TILE(16, 4) }
+    else if (rem >= 8) { TILE(8, 4) }
+    else if (rem >= 4) { TILE(4, 8) }
+    else if (rem >= 2) { TILE(2, 8) }
+    else { TILE(1, 8) }
+#undef TILE
+  }
+  return e;
+}
+
+}  // namespace
+}  // namespace inch
+
+using namespace inch;
+
+extern "C" size_t inch_spmm_workspace_size(int64_t n_atoms, int32_t b, int32_t r) {
+  (void)n_atoms;
+  (void)b;
+  Sizer s;
+  s.take<double>((size_t)kQxBlocks * 8 * 16);  // partial sums (r <= 8, tile <= 16)
+  s.take<double>(8 * 16);                      // coefficients
+  (void)r;
+  return s.bytes();
+}
+
+extern "C" inch_status inch_spmm(int32_t prec, int64_t n_atoms, const int64_t* rowptr, const void* ent,
+                                 const void* diag, const void* X, int64_t ldx, int32_t b, void* Y, int64_t ldy,
+                                 const void* Yin, int64_t ldyin, void* Acc, int64_t ldacc, const double* q,
+                                 const inch_spmm_epilogue* ep_in, void* ws, size_t ws_bytes, cudaStream_t stream) {
+  INCH_REQUIRE(prec == 32 || prec == 64, INCH_INVALID_ARG, "inch_spmm: prec must be 32 or 64");
+  INCH_REQUIRE(rowptr && ent && diag && X && Y && ep_in, INCH_INVALID_ARG, "inch_spmm: NULL argument");
+  INCH_REQUIRE(n_atoms >= 1 && n_atoms < (int64_t(1) << 31), INCH_INVALID_ARG, "inch_spmm: n_atoms out of range");
+  INCH_REQUIRE(b >= 1 && b <= 64, INCH_INVALID_ARG, "inch_spmm: b=%d outside 1..64", b);
+  INCH_REQUIRE(ldx >= b && ldy >= b, INCH_INVALID_ARG, "inch_spmm: leading dimension below b");
+  INCH_REQUIRE(X != Y, INCH_INVALID_ARG, "inch_spmm: X and Y must not alias");
+  const inch_spmm_epilogue& e = *ep_in;
+  INCH_REQUIRE(e.r >= 0 && e.r <= 8, INCH_INVALID_ARG, "inch_spmm: deflation rank %d outside 0..8", e.r);
+  INCH_REQUIRE(e.r == 0 || q != nullptr, INCH_INVALID_ARG, "inch_spmm: deflation basis is NULL");
+  INCH_REQUIRE(e.beta == 0.0 || (Yin != nullptr && ldyin >= b), INCH_INVALID_ARG, "inch_spmm: beta != 0 needs Yin");
+  INCH_REQUIRE(!e.accumulate || (Acc != nullptr && ldacc >= b), INCH_INVALID_ARG, "inch_spmm: accumulate needs Acc");
+  INCH_REQUIRE(((uintptr_t)ent & 15) == 0 && ((uintptr_t)diag & 15) == 0, INCH_INVALID_ARG,
+               "inch_spmm: store buffers must be 16-byte aligned");
+  double *partial = nullptr, *coef = nullptr;
+  if (e.r > 0) {
+    Carver c(ws, ws_bytes);
+    partial = c.take<double>((size_t)kQxBlocks * 8 * 16);
+    coef = c.take<double>(8 * 16);
+    INCH_REQUIRE(c.ok, INCH_OOM, "inch_spmm: workspace of %zu bytes, need %zu", ws_bytes,
+                 inch_spmm_workspace_size(n_atoms, b, e.r));
+  }
+  Epi ep{e.alpha, e.gamma, e.beta, e.mu, e.r, e.accumulate, (e.beta != 0.0) ? 1 : 0};
+  cudaError_t err;
+  if (prec == 32)
+    err = run<float>(n_atoms, rowptr, ent, diag, X, ldx, b, Y, ldy, Yin, ldyin, Acc, ldacc, ep, q, e.hot_shift,
+                     partial, coef, stream);
+  else
+    err = run<double>(n_atoms, rowptr, ent, diag, X, ldx, b, Y, ldy, Yin, ldyin, Acc, ldacc, ep, q, e.hot_shift,
+                      partial, coef, stream);
+  INCH_REQUIRE(err == cudaSuccess, INCH_CUDA_ERROR, "inch_spmm: %s", cudaGetErrorString(err));
+  return INCH_OK;
+}

@@ -1,0 +1,113 @@
+"""The block-banded ANM Hessian store and its operator.
+
+`HessianStore` stands where the reference returns its lower-triangle CuPy CSR
+matrix (InchingLiteInteger/Fuel/T1.py:655-660): it has ``shape``, ``dtype`` and
+``ndim`` (the solvers' argument checks read them, e.g. ThickRestartLanczos.../
+T1.py:85-87) and holds, on the GPU, the Cuthill-McKee-banded adjacency and the
+rank-one block store (w = x/|x| per pair, symmetric diagonal blocks) in FP64
+and/or FP32.  Products go through the fused SpMM kernel.
+"""
+from __future__ import annotations
+
+import numpy as np
+import torch
+
+from . import _native, graph
+
+
+class HessianStore:
+    """ANM Hessian H + PlusI*I of a structure whose atoms are already in the
+    order the caller wants (normally reversed Cuthill-McKee)."""
+
+    def __init__(self, X_nm, rc_gamma_A: float = 8.0, plus_i: float = 1.0, precisions=("f64", "f32"),
+                 device=None, graph_=None):
+        self.X = graph.to_device_coords(X_nm, device)
+        self.device = self.X.device
+        self.n_atoms = int(self.X.shape[0])
+        self.rc_nm = rc_gamma_A / 10.0
+        self.plus_i = float(plus_i)
+        if graph_ is None:
+            graph_ = _native.neighbor_lists(self.X, self.rc_nm)
+        self.degree, self.rowptr, self.cols = graph_
+        want64 = "f64" in precisions
+        want32 = "f32" in precisions
+        self.ent64, self.diag64, self.ent32, self.diag32 = _native.hessian_assemble(
+            self.X, self.rowptr, self.cols, self.rc_nm, self.plus_i, want64, want32)
+        n = 3 * self.n_atoms
+        self.shape = (n, n)
+        self.ndim = 2
+        self.dtype = np.dtype(np.float64)
+        self.nnz_blocks = int(self.cols.shape[0])
+        self._diag_vec = None
+
+    # -- reference-compatible views ------------------------------------------------
+    @property
+    def A_diag(self) -> torch.Tensor:
+        """Diagonal of H + PlusI*I, (3N,) float64 (what the reference returns beside A)."""
+        if self._diag_vec is None:
+            d = self.diag64 if self.diag64 is not None else self.diag32.double()
+            self._diag_vec = d[:, :3].reshape(-1).contiguous()
+        return self._diag_vec
+
+    def has(self, prec: int) -> bool:
+        return (self.ent64 if prec == 64 else self.ent32) is not None
+
+    def store(self, prec: int):
+        if prec == 64:
+            if self.ent64 is None:
+                raise AssertionError("ABORTED. the FP64 store was not assembled")
+            return self.ent64, self.diag64
+        if self.ent32 is None:
+            raise AssertionError("ABORTED. the FP32 store was not assembled")
+        return self.ent32, self.diag32
+
+    def store_bytes(self, prec: int) -> int:
+        """Bytes one SpMM pass streams from the store (entries + diagonal + rowptr)."""
+        ent, diag = self.store(prec)
+        return ent.numel() * ent.element_size() + diag.numel() * diag.element_size() + 8 * (self.n_atoms + 1)
+
+    # -- products ---------------------------------------------------------------
+    def matmul(self, X, out=None, prec=None, **epilogue):
+        """out = H X (+ fused epilogue, see _native.spmm).  prec defaults to X's dtype."""
+        if prec is None:
+            prec = 64 if X.dtype == torch.float64 else 32
+        want = torch.float64 if prec == 64 else torch.float32
+        if X.dtype != want:
+            raise AssertionError(f"ABORTED. prec {prec} needs {want} vectors, got {X.dtype}")
+        if out is None:
+            out = torch.empty_like(X)
+        ent, diag = self.store(prec)
+        return _native.spmm(prec, self.n_atoms, self.rowptr, ent, diag, X, out, **epilogue)
+
+    def __matmul__(self, X):
+        return self.matmul(X)
+
+    # -- test helpers ---------------------------------------------------------------
+    def to_scipy_lower(self):
+        """Lower triangle (incl. diagonal) as scipy CSR, FP64 (for tests only)."""
+        import scipy.sparse as sp
+        n = self.n_atoms
+        rowptr = self.rowptr.cpu().numpy()
+        cols = self.cols.cpu().numpy().astype(np.int64)
+        ent = (self.ent64 if self.ent64 is not None else self.ent32.double()).cpu().numpy()
+        diag = (self.diag64 if self.diag64 is not None else self.diag32.double()).cpu().numpy()
+        rows = np.repeat(np.arange(n), np.diff(rowptr))
+        w = ent[:, :3]
+        blocks = -w[:, :, None] * w[:, None, :]
+        D = np.zeros((n, 3, 3))
+        D[:, 0, 0], D[:, 1, 1], D[:, 2, 2] = diag[:, 0], diag[:, 1], diag[:, 2]
+        D[:, 0, 1] = D[:, 1, 0] = diag[:, 3]
+        D[:, 0, 2] = D[:, 2, 0] = diag[:, 4]
+        D[:, 1, 2] = D[:, 2, 1] = diag[:, 5]
+        off = rows != cols
+        bi = np.concatenate([rows[off], np.arange(n)])
+        bj = np.concatenate([cols[off], np.arange(n)])
+        bv = np.concatenate([blocks[off], D])
+        p, q = np.meshgrid(np.arange(3), np.arange(3), indexing="ij")
+        R = (3 * bi[:, None, None] + p[None]).ravel()
+        C = (3 * bj[:, None, None] + q[None]).ravel()
+        V = bv.ravel()
+        keep = (C <= R) & (V != 0.0)
+        A = sp.csr_matrix((V[keep], (R[keep], C[keep])), shape=self.shape)
+        A.sum_duplicates()
+        return A

@@ -1,0 +1,172 @@
+/*
+ * inching_b200 C ABI: B200-native kernels for the Inching normal-mode hot path
+ * (ANM Hessian build, Cuthill-McKee banding, Hessian x multivector products).
+ *
+ * Conventions
+ *   - Every pointer argument named *_dev is device memory (cudaMalloc'd or a torch
+ *     tensor's data_ptr); *_host is host memory.
+ *   - Every entry point takes the cudaStream_t it enqueues on.  Entry points that
+ *     must read a size back to the host say "synchronises" and do so on that stream.
+ *   - The library never frees caller memory and never allocates device memory:
+ *     scratch comes from a caller-provided workspace whose size is queried first.
+ *   - Return value: INCH_OK or an error code; inch_last_error_string() gives a
+ *     message for the calling thread's last error.
+ *   - Coordinates are float64 nanometres, atoms in caller order; degrees of
+ *     freedom are dof = 3*atom + axis.
+ *
+ * Reference interfaces replaced (paths inside jhmlam/Inching):
+ *   inch_neighbors_*  -> cKDTree.query_ball_point in X_KdCuthillMckeeOrder /
+ *                        X_KdUngappedMinMaxNeighbor (InchingLiteInteger/Fuel/Coordinate/T1.py:218-245,397)
+ *   inch_rcm          -> the BFS of X_KdCuthillMckeeOrder (Fuel/Coordinate/T1.py:254-323)
+ *   inch_band_slices  -> the gap scan of X_KdUngappedMinMaxNeighbor (Fuel/Coordinate/T1.py:371-481)
+ *   inch_hessian_assemble -> Xnumpy_SparseCupyMatrixUngappped.ReturnCupyHLowerTriangleInt32/64
+ *                        (InchingLiteInteger/Fuel/T1.py:228-660, 666-1048)
+ *   inch_spmm         -> OOC2_HalfMemS_v_KrylovAv_VOID / OOC2_FullMemS_v_KrylovAv_VOID
+ *                        (InchingLiteInteger/Burn/Krylov/T3.py:54-239), with the Hotelling update
+ *                        of Burn/Orthogonalization/T3.py:62-164 and one step of the Chebyshev
+ *                        recurrence of Burn/PolynomialFilters/T2.py:59-80 fused in its epilogue
+ */
+#ifndef INCHING_B200_H
+#define INCHING_B200_H
+
+#include <stddef.h>
+#include <stdint.h>
+#include <cuda_runtime.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+typedef enum {
+  INCH_OK = 0,
+  INCH_INVALID_ARG = 1,
+  INCH_OOM = 2,            /* workspace too small */
+  INCH_NOT_CONVERGED = 3,
+  INCH_TIMEOUT = 4,
+  INCH_CUDA_ERROR = 5,
+  INCH_LIMIT = 6           /* an input exceeds a documented kernel limit */
+} inch_status;
+
+/* Message for the calling thread's most recent error ("" if none). */
+const char* inch_last_error_string(void);
+/* ABI version of this library (bumped on any signature change). */
+int inch_abi_version(void);
+
+/* ---------------------------------------------------------------------------
+ * Cell-list neighbour search.  j is a neighbour of i iff
+ *   ((dx*dx) + dy*dy) + dz*dz <= rc*rc   (each step rounded to double, no FMA),
+ * the distance rule of scipy cKDTree.query_ball_point(p=2, eps=0) used by the
+ * reference.  Lists include i itself and are sorted ascending.
+ * ------------------------------------------------------------------------- */
+typedef struct {
+  double origin[3];      /* lower corner of the cell grid (nm) */
+  double cell;           /* cell edge (nm), >= rc */
+  int32_t dims[3];       /* cells per axis */
+  int64_t ncells;
+  int64_t n_atoms;
+} inch_cell_grid;
+
+/* Bounding box of X_dev (N,3) -> grid with cell edge rc.  Needs 64 bytes of
+ * workspace.  Synchronises the stream.  Replaces the cKDTree construction of
+ * Fuel/Coordinate/T1.py:218-226. */
+inch_status inch_cell_grid_plan(const double* X_dev, int64_t n_atoms, double rc,
+                                inch_cell_grid* grid_host, void* ws_dev, size_t ws_bytes,
+                                cudaStream_t stream);
+
+/* Workspace bytes for inch_neighbors_count / inch_neighbors_fill on this grid. */
+size_t inch_neighbors_workspace_size(const inch_cell_grid* grid_host);
+
+/* Builds the cell list in the workspace, writes degree_dev[N] (neighbours incl.
+ * self) and rowptr_dev[N+1] (exclusive prefix sum, int64), and copies the total
+ * neighbour count to *nnz_host.  Synchronises the stream.
+ * Replaces the degree pass of Fuel/Coordinate/T1.py:236-245. */
+inch_status inch_neighbors_count(const double* X_dev, const inch_cell_grid* grid_host, double rc,
+                                 int32_t* degree_dev, int64_t* rowptr_dev, int64_t* nnz_host,
+                                 void* ws_dev, size_t ws_bytes, cudaStream_t stream);
+
+/* Fills cols_dev[nnz] with the sorted neighbour lists.  Must follow
+ * inch_neighbors_count with the same workspace (the cell list is reused).
+ * At most INCH_MAX_DEGREE neighbours per atom (else INCH_LIMIT).  Synchronises.
+ * Replaces query_ball_point(..., return_sorted=True) (Fuel/Coordinate/T1.py:276,397). */
+#define INCH_MAX_DEGREE 1024
+inch_status inch_neighbors_fill(const double* X_dev, const inch_cell_grid* grid_host, double rc,
+                                const int64_t* rowptr_dev, int32_t* cols_dev,
+                                void* ws_dev, size_t ws_bytes, cudaStream_t stream);
+
+/* ---------------------------------------------------------------------------
+ * Cuthill-McKee ordering (level-synchronous, bit-exact with the sequential BFS
+ * of Fuel/Coordinate/T1.py:254-323).  seed_order_dev is np.argsort(degree) as
+ * computed by the reference (its tie order is the caller's numpy's); the next
+ * unvisited atom in that order seeds each connected component.
+ * Outputs the REVERSED order (rcm_order_dev, int64 N) and its inverse
+ * (undo_dev, int64 N), as X_KdCuthillMckeeOrder(..., Reverse=True) returns.
+ * Synchronises once per BFS level.
+ * ------------------------------------------------------------------------- */
+size_t inch_rcm_workspace_size(int64_t n_atoms);
+inch_status inch_rcm(const int64_t* rowptr_dev, const int32_t* cols_dev, const int32_t* degree_dev,
+                     const int64_t* seed_order_dev, int64_t n_atoms,
+                     int64_t* rcm_order_dev, int64_t* undo_dev, int32_t* n_levels_host,
+                     void* ws_dev, size_t ws_bytes, cudaStream_t stream);
+
+/* ---------------------------------------------------------------------------
+ * Ungapped band slices of X_KdUngappedMinMaxNeighbor (Fuel/Coordinate/T1.py:371-481)
+ * from the adjacency of the (reordered) structure.  batch_head_dev holds
+ * n_batches+1 row heads.  For batch b, slices are written to
+ * starts/ends[b*max_slices ...] and their number to counts_dev[b].  *total_nbrs_host
+ * receives the sum of all degrees (for HalfNnz).  A batch with more than
+ * max_slices slices, or more than 2048 gaps wider than `gap`, returns INCH_LIMIT.
+ * nnz = rowptr[n_atoms] < 2^31.  Synchronises.
+ * ------------------------------------------------------------------------- */
+size_t inch_band_slices_workspace_size(int64_t n_batches, int64_t nnz);
+inch_status inch_band_slices(const int64_t* rowptr_dev, const int32_t* cols_dev, int64_t n_atoms,
+                             const int64_t* batch_head_dev, int64_t n_batches, int64_t gap,
+                             int32_t max_slices, int64_t* starts_dev, int64_t* ends_dev,
+                             int32_t* counts_dev, int64_t* total_nbrs_host,
+                             void* ws_dev, size_t ws_bytes, cudaStream_t stream);
+
+/* ---------------------------------------------------------------------------
+ * ANM Hessian store.  Off-diagonal block (i,j) = -(x x^T)/d^2 for 0 < d^2 <= rc^2,
+ * x = X_j - X_i, is rank one: it is stored as w = x/d, so block = -w w^T.
+ * Diagonal block (i,i) = sum_j w w^T + plus_i * I, stored as 6 unique values
+ * (xx, yy, zz, xy, xz, yz) padded to 8.
+ *   entries: one per adjacency entry (self included, w = 0 there), same order
+ *            as cols: f64 layout {wx, wy, wz, (double)col} (32 B),
+ *            f32 layout {wx, wy, wz, col bits} (16 B).
+ *   diag:    f64 (N,8) and f32 (N,8).
+ * Pass NULL for a precision that is not wanted.
+ * Replaces Fuel/T1.py:276-455 (pair blocks, diagonal row sum, +PlusI).
+ * ------------------------------------------------------------------------- */
+inch_status inch_hessian_assemble(const double* X_dev, int64_t n_atoms, double rc, double plus_i,
+                                  const int64_t* rowptr_dev, const int32_t* cols_dev,
+                                  double* ent64_dev, double* diag64_dev,
+                                  float* ent32_dev, float* diag32_dev, cudaStream_t stream);
+
+/* ---------------------------------------------------------------------------
+ * Hessian x multivector with fused epilogue.  X and Y are (3N, b) row-major with
+ * leading dimension ld (>= b), element (dof, c) at dof*ld + c.
+ *   Y = alpha*(H X) + gamma*X + beta*Yin + hot_shift * Q^T (Q X)   [Acc += mu*Y]
+ * where Q is the (r, 3N) row-major FP64 deflation basis (r <= 8; explicit
+ * Hotelling deflation); its coefficients Q X are reduced inside the call.
+ * Yin may alias Y.  prec: 64 -> f64 store and f64 vectors; 32 -> f32 store and
+ * f32 vectors.  Supported b: 1..64 (f32) / 1..32 (f64).
+ * ------------------------------------------------------------------------- */
+typedef struct {
+  double alpha, gamma, beta, mu, hot_shift;
+  int32_t r;              /* deflation rank (0 = none) */
+  int32_t accumulate;     /* 1 -> Acc += mu*Y */
+} inch_spmm_epilogue;
+
+size_t inch_spmm_workspace_size(int64_t n_atoms, int32_t b, int32_t r);
+inch_status inch_spmm(int32_t prec, int64_t n_atoms, const int64_t* rowptr_dev,
+                      const void* ent_dev, const void* diag_dev,
+                      const void* X_dev, int64_t ldx, int32_t b,
+                      void* Y_dev, int64_t ldy, const void* Yin_dev, int64_t ldyin,
+                      void* Acc_dev, int64_t ldacc,
+                      const double* q_dev /* (r, 3N) row-major, FP64 */,
+                      const inch_spmm_epilogue* ep,
+                      void* ws_dev, size_t ws_bytes, cudaStream_t stream);
+
+#ifdef __cplusplus
+}
+#endif
+#endif /* INCHING_B200_H */

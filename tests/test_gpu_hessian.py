@@ -1,0 +1,109 @@
+"""GPU parity of the Hessian store and the fused SpMM against the FP64 oracle
+(restatement of Fuel/T1.py:276-455 and Krylov/T3.py:128-160).
+
+Tolerances: FP64 store/products 1e-12 relative to ||H||; FP32 store/products
+2e-6 relative to ||H|| (single-precision rounding of w and of the sums)."""
+import numpy as np
+import pytest
+import torch
+
+from oracle import hessian as oh
+
+pytestmark = pytest.mark.gpu
+
+TOL64 = 1e-12
+TOL32 = 2e-6
+
+
+@pytest.fixture(scope="module")
+def case():
+    from inching_b200 import graph, synth
+    from inching_b200.hessian import HessianStore
+    X = synth.globule(1500, seed=7) / 10.0
+    order, undo = graph.cuthill_mckee(X, 8.0)
+    Xr = X[order.cpu().numpy()]
+    H = HessianStore(Xr, 8.0, plus_i=1.0)
+    A, Ad = oh.hessian_lower(Xr, 8.0, 1.0)
+    Hfull = oh.full_from_lower(A, Ad)
+    Q = oh.rigid_body_basis(Xr)
+    return Xr, H, A, Ad, Hfull, Q
+
+
+def test_store_matches_oracle(case):
+    Xr, H, A, Ad, Hfull, Q = case
+    L = H.to_scipy_lower()
+    scale = abs(Hfull).max()
+    diff = abs(L - A)
+    assert diff.max() <= TOL64 * scale
+    assert np.allclose(H.A_diag.cpu().numpy(), Ad, rtol=0, atol=TOL64 * scale)
+
+
+def test_rigid_body_null_space_and_symmetry(case):
+    Xr, H, A, Ad, Hfull, Q = case
+    Qt = torch.from_numpy(Q.T.copy()).cuda()
+    Y = H.matmul(Qt)
+    assert torch.allclose(Y, Qt * H.plus_i, atol=1e-12, rtol=0)
+    v = torch.randn(H.shape[0], 2, dtype=torch.float64, device="cuda")
+    Hv = H.matmul(v.contiguous())
+    assert abs(float(v[:, 0] @ Hv[:, 1] - v[:, 1] @ Hv[:, 0])) < 1e-10
+
+
+@pytest.mark.parametrize("b", [1, 2, 3, 8, 13, 16, 40])
+@pytest.mark.parametrize("prec", [64, 32])
+def test_spmm_matches_krylov_av(case, b, prec):
+    Xr, H, A, Ad, Hfull, Q = case
+    if prec == 64 and b > 32:
+        pytest.skip("FP64 tiles up to 32 columns per call are exercised")
+    rng = np.random.default_rng(b)
+    Xv = rng.standard_normal((H.shape[0], b))
+    ref = np.stack([oh.krylov_av(A, Ad, Xv[:, c]) for c in range(b)], axis=1)
+    dt = torch.float64 if prec == 64 else torch.float32
+    Xt = torch.from_numpy(Xv).to("cuda", dt)
+    if b == 1:
+        Xt = Xt[:, 0].contiguous()
+        ref = ref[:, 0]
+    Y = H.matmul(Xt, prec=prec)
+    tol = (TOL64 if prec == 64 else TOL32) * abs(Hfull).max() * np.abs(Xv).max() * 10
+    assert np.abs(Y.double().cpu().numpy() - ref).max() <= tol
+
+
+@pytest.mark.parametrize("prec", [64, 32])
+def test_spmm_fused_epilogue(case, prec):
+    """Y = a*HX + g*X + b*Yin + s*Q^T Q X and Acc += mu*Y in one call, vs the oracle
+    composition (Krylov/T3.py + Orthogonalization/T3.py + PolynomialFilters/T2.py)."""
+    Xr, H, A, Ad, Hfull, Q = case
+    b = 4
+    rng = np.random.default_rng(3)
+    Xv = rng.standard_normal((H.shape[0], b))
+    Yin = rng.standard_normal((H.shape[0], b))
+    Acc0 = rng.standard_normal((H.shape[0], b))
+    a, g, be, s, mu = 0.37, -1.25, -1.0, 10.0, 0.6
+    HX = np.stack([oh.krylov_av(A, Ad, Xv[:, c]) for c in range(b)], axis=1)
+    ref = a * HX + g * Xv + be * Yin + s * Q.T @ (Q @ Xv)
+    dt = torch.float64 if prec == 64 else torch.float32
+    t = lambda m: torch.from_numpy(m).to("cuda", dt).contiguous()
+    Xt, Yt, Acc = t(Xv), t(Yin), t(Acc0)
+    Qd = torch.from_numpy(Q).cuda()
+    H.matmul(Xt, out=Yt, prec=prec, alpha=a, gamma=g, beta=be, Yin=Yt, acc=Acc, mu=mu, Q=Qd, hot_shift=s)
+    tol = (TOL64 if prec == 64 else TOL32) * abs(Hfull).max() * 50
+    assert np.abs(Yt.double().cpu().numpy() - ref).max() <= tol
+    assert np.abs(Acc.double().cpu().numpy() - (Acc0 + mu * ref)).max() <= tol
+
+
+def test_full_size_store_properties():
+    """100,000-atom assembly: symmetry via random bilinear forms and the six
+    rigid-body vectors as exact eigenvectors (H q = PlusI q), FP64 and FP32."""
+    from inching_b200 import graph, synth
+    from inching_b200.hessian import HessianStore
+    X = synth.workload("assembly100k") / 10.0
+    order, _ = graph.cuthill_mckee(X, 8.0)
+    Xr = X[order.cpu().numpy()]
+    H = HessianStore(Xr, 8.0, plus_i=1.0)
+    Q = torch.from_numpy(oh.rigid_body_basis(Xr).T.copy()).cuda()
+    Y = H.matmul(Q)
+    assert (Y - Q).abs().max().item() < 1e-11
+    Y32 = H.matmul(Q.float().contiguous(), prec=32)
+    assert (Y32.double() - Q).abs().max().item() < 1e-4
+    v = torch.randn(H.shape[0], 2, dtype=torch.float64, device="cuda").contiguous()
+    Hv = H.matmul(v)
+    assert abs(float(v[:, 0] @ Hv[:, 1] - v[:, 1] @ Hv[:, 0])) < 1e-8 * float(v[:, 0] @ Hv[:, 0])
