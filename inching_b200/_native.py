@@ -37,6 +37,15 @@ class SpmmEpilogue(Structure):
 
 _lib = None
 
+# Running count of kernels this binding has launched (each wrapper adds the
+# number of kernels its entry point enqueues); read by measurement code.
+launches = 0
+
+
+def _count(n):
+    global launches
+    launches += int(n)
+
 # name -> (restype, argtypes)
 _SIGS = {
     "inch_last_error_string": (c_char_p, []),
@@ -136,6 +145,7 @@ def neighbor_lists(X: torch.Tensor, rc_nm: float):
     cols = torch.empty(max(nnz.value, 1), dtype=torch.int32, device=dev)[:nnz.value]
     check(L.inch_neighbors_fill(_ptr(X), ctypes.byref(grid), rc_nm, _ptr(rowptr), _ptr(cols),
                                 _ptr(ws), ws.numel(), _stream()))
+    _count(8)   # bbox, assign, scan, scatter, count, set0, scan, fill
     return degree, rowptr, cols
 
 
@@ -153,6 +163,7 @@ def cuthill_mckee(rowptr, cols, degree, seed_order):
     levels = c_int32(0)
     check(L.inch_rcm(_ptr(rowptr), _ptr(cols), _ptr(degree), _ptr(seed_order), n, _ptr(order), _ptr(undo),
                      ctypes.byref(levels), _ptr(ws), ws.numel(), _stream()))
+    _count(5 + 5 * levels.value)
     return order, undo, levels.value
 
 
@@ -191,6 +202,7 @@ def hessian_assemble(X, rowptr, cols, rc_nm, plus_i, want64=True, want32=True):
     diag32 = torch.empty((n, 8), dtype=torch.float32, device=dev) if want32 else None
     check(lib().inch_hessian_assemble(_ptr(X), n, rc_nm, plus_i, _ptr(rowptr), _ptr(cols), _ptr(ent64),
                                       _ptr(diag64), _ptr(ent32), _ptr(diag32), _stream()))
+    _count(1)
     return ent64, diag64, ent32, diag32
 
 
@@ -219,4 +231,11 @@ def spmm(prec, n_atoms, rowptr, ent, diag, X, Y, *, alpha=1.0, gamma=0.0, beta=0
     check(L.inch_spmm(prec, n_atoms, _ptr(rowptr), _ptr(ent), _ptr(diag), _ptr(X), ldx, b, _ptr(Y), ldy,
                       _ptr(Yin), ldyin, _ptr(acc), ldacc, _ptr(Q), ctypes.byref(ep), _ptr(ws), ws.numel(),
                       _stream()))
+    tiles = 0
+    rem = b
+    for t in ((64, 32, 16, 8, 4, 2, 1) if prec == 32 else (32, 16, 8, 4, 2, 1)):
+        while rem >= t:
+            rem -= t
+            tiles += 1
+    _count(tiles * (3 if r > 0 else 1))
     return Y

@@ -117,13 +117,81 @@ k_spmm(int64_t n_atoms, const int64_t* __restrict__ rowptr, const void* __restri
   }
 }
 
+// Wide multivectors: lanes map to columns.  A group of LPR = min(B, 32) lanes
+// owns one row; every lane of the group reads the same 16-byte entry (one
+// broadcast transaction) and the group reads each X_j row as one coalesced
+// segment, so gathers cost 3 warp-wide loads per entry instead of 3*B scalar
+// loads per lane.  No shuffles: each lane accumulates its own columns.
+template <class T, int B>
+__global__ void __launch_bounds__(kThreads)
+k_spmm_cols(int64_t n_atoms, const int64_t* __restrict__ rowptr, const void* __restrict__ ent,
+            const T* __restrict__ diag, const T* __restrict__ X, int64_t ldx, T* Y, int64_t ldy, const T* Yin,
+            int64_t ldyin, T* __restrict__ Acc, int64_t ldacc, int c0, Epi ep, const double* __restrict__ Q,
+            int64_t ndof, const double* __restrict__ coef) {
+  constexpr int LPR = B < 32 ? B : 32;
+  constexpr int CPL = B / LPR;
+  constexpr int RPW = 32 / LPR;
+  constexpr int RPB = (kThreads / 32) * RPW;
+  __shared__ double s_coef[8 * B];
+  if (ep.r > 0) {
+    for (int t = threadIdx.x; t < ep.r * B; t += kThreads) s_coef[t] = coef[t];
+    __syncthreads();
+  }
+  const int lane = threadIdx.x & 31;
+  const int cl = lane % LPR;
+  const int64_t first = (int64_t)blockIdx.x * RPB + (threadIdx.x >> 5) * RPW + lane / LPR;
+  for (int64_t i = first; i < n_atoms; i += (int64_t)gridDim.x * RPB) {
+    T acc[3][CPL];
+#pragma unroll
+    for (int t = 0; t < CPL; ++t) acc[0][t] = acc[1][t] = acc[2][t] = T(0);
+    const int64_t e1 = rowptr[i + 1];
+    const T* Xc = X + c0 + cl;
+#pragma unroll 4
+    for (int64_t e = rowptr[i]; e < e1; ++e) {
+      T wx, wy, wz;
+      int j;
+      Ent<T>::load(ent, e, wx, wy, wz, j);
+      const T* xj = Xc + 3 * (int64_t)j * ldx;
+#pragma unroll
+      for (int t = 0; t < CPL; ++t) {
+        const T x0 = __ldg(xj + t * LPR), x1 = __ldg(xj + ldx + t * LPR), x2 = __ldg(xj + 2 * ldx + t * LPR);
+        const T dot = wx * x0 + wy * x1 + wz * x2;
+        acc[0][t] -= wx * dot;
+        acc[1][t] -= wy * dot;
+        acc[2][t] -= wz * dot;
+      }
+    }
+    const T* d = diag + 8 * i;
+    const T dxx = d[0], dyy = d[1], dzz = d[2], dxy = d[3], dxz = d[4], dyz = d[5];
+    const int64_t r0 = 3 * i;
+#pragma unroll
+    for (int t = 0; t < CPL; ++t) {
+      const int c = cl + t * LPR;
+      const T x0 = X[r0 * ldx + c0 + c], x1 = X[(r0 + 1) * ldx + c0 + c], x2 = X[(r0 + 2) * ldx + c0 + c];
+      T h[3];
+      h[0] = acc[0][t] + dxx * x0 + dxy * x1 + dxz * x2;
+      h[1] = acc[1][t] + dxy * x0 + dyy * x1 + dyz * x2;
+      h[2] = acc[2][t] + dxz * x0 + dyz * x1 + dzz * x2;
+      const T xs[3] = {x0, x1, x2};
+#pragma unroll
+      for (int a = 0; a < 3; ++a) {
+        const int64_t row = r0 + a;
+        double y = ep.alpha * (double)h[a] + ep.gamma * (double)xs[a];
+        if (ep.has_yin) y += ep.beta * (double)Yin[row * ldyin + c0 + c];
+        for (int q = 0; q < ep.r; ++q) y += Q[q * ndof + row] * s_coef[q * B + c];
+        Y[row * ldy + c0 + c] = (T)y;
+        if (ep.accumulate) Acc[row * ldacc + c0 + c] += (T)(ep.mu * y);
+      }
+    }
+  }
+}
+
 // Partial sums of Q X over a dof range (blockIdx.x), one deflation vector per
 // blockIdx.y; thread t accumulates column t % B.
 template <class T, int B>
 __global__ void __launch_bounds__(kThreads)
 k_qx_partial(const double* __restrict__ Q, int64_t ndof, const T* __restrict__ X, int64_t ldx, int c0,
              double* __restrict__ partial) {
-  __shared__ double s[kThreads / 32][32];
   const int q = blockIdx.y, r = gridDim.y;
   const double* qr = Q + q * ndof;
   const int c = threadIdx.x % B;
@@ -133,22 +201,19 @@ k_qx_partial(const double* __restrict__ Q, int64_t ndof, const T* __restrict__ X
     const int64_t dof = p / B;
     acc += qr[dof] * (double)X[dof * ldx + c0 + c];
   }
-#pragma unroll
-  for (int o = 16; o >= B; o >>= 1) acc += __shfl_xor_sync(0xffffffffu, acc, o);
-  const int lane = threadIdx.x & 31, w = threadIdx.x >> 5;
-  if (lane < B) s[w][lane] = acc;
+  __shared__ double s[kThreads];
+  s[threadIdx.x] = acc;
   __syncthreads();
   if (threadIdx.x < B) {
     double t = 0.0;
-    for (int k = 0; k < kThreads / 32; ++k) t += s[k][threadIdx.x];
+    for (int u = threadIdx.x; u < kThreads; u += B) t += s[u];
     partial[((int64_t)blockIdx.x * r + q) * B + threadIdx.x] = t;
   }
 }
 
 __global__ void k_qx_final(const double* __restrict__ partial, int P, int r, int B, double shift,
                            double* __restrict__ coef) {
-  const int t = threadIdx.x;
-  if (t < r * B) {
+  for (int t = threadIdx.x; t < r * B; t += blockDim.x) {
     double s = 0.0;
     for (int p = 0; p < P; ++p) s += partial[(int64_t)p * r * B + t];
     coef[t] = shift * s;
@@ -166,12 +231,20 @@ cudaError_t launch_tile(int64_t n_atoms, const int64_t* rowptr, const void* ent,
   if (ep.r > 0) {
     dim3 g(kQxBlocks, ep.r);
     k_qx_partial<T, B><<<g, kThreads, 0, stream>>>(Q, ndof, X, ldx, c0, partial);
-    k_qx_final<<<1, 256, 0, stream>>>(partial, kQxBlocks, ep.r, B, hot_shift, coef);
+    k_qx_final<<<1, 512, 0, stream>>>(partial, kQxBlocks, ep.r, B, hot_shift, coef);
   }
-  const int rows_per_block = kThreads / G;
-  const int blocks = grid_for(n_atoms, rows_per_block, 148 * 16);
-  k_spmm<T, B, G><<<blocks, kThreads, 0, stream>>>(n_atoms, rowptr, ent, diag, X, ldx, Y, ldy, Yin, ldyin, Acc,
-                                                   ldacc, c0, ep, Q, ndof, coef);
+  if constexpr (G == 0) {
+    constexpr int LPR = B < 32 ? B : 32;
+    const int rows_per_block = (kThreads / 32) * (32 / LPR);
+    const int blocks = grid_for(n_atoms, rows_per_block, 148 * 64);
+    k_spmm_cols<T, B><<<blocks, kThreads, 0, stream>>>(n_atoms, rowptr, ent, diag, X, ldx, Y, ldy, Yin, ldyin, Acc,
+                                                       ldacc, c0, ep, Q, ndof, coef);
+  } else {
+    const int rows_per_block = kThreads / G;
+    const int blocks = grid_for(n_atoms, rows_per_block, 148 * 16);
+    k_spmm<T, B, G><<<blocks, kThreads, 0, stream>>>(n_atoms, rowptr, ent, diag, X, ldx, Y, ldy, Yin, ldyin, Acc,
+                                                     ldacc, c0, ep, Q, ndof, coef);
+  }
   return cudaGetLastError();
 }
 
@@ -192,8 +265,10 @@ cudaError_t run(int64_t n_atoms, const int64_t* rowptr, const void* ent, const v
   e = launch_tile<T, BB, GG>(n_atoms, rowptr, ent, D, X, ldx, Y, ldy, Yin, ldyin, Acc, ldacc, c0, ep, Q,     \
                              hot_shift, partial, coef, s);                                                     \
   c0 += BB;
-    if (rem >= 16 && sizeof(T) == 4) { TILE(16, 4) }
-    else if (rem >= 8) { TILE(8, 4) }
+    if (rem >= 64 && sizeof(T) == 4) { TILE(64, 0) }
+    else if (rem >= 32) { TILE(32, 0) }
+    else if (rem >= 16) { TILE(16, 0) }
+    else if (rem >= 8) { TILE(8, 0) }
     else if (rem >= 4) { TILE(4, 8) }
     else if (rem >= 2) { TILE(2, 8) }
     else { TILE(1, 8) }
@@ -211,8 +286,8 @@ extern "C" size_t inch_spmm_workspace_size(int64_t n_atoms, int32_t b, int32_t r
   (void)n_atoms;
   (void)b;
   Sizer s;
-  s.take<double>((size_t)kQxBlocks * 8 * 16);  // partial sums (r <= 8, tile <= 16)
-  s.take<double>(8 * 16);                      // coefficients
+  s.take<double>((size_t)kQxBlocks * 8 * 64);  // partial sums (r <= 8, tile <= 64)
+  s.take<double>(8 * 64);                      // coefficients
   (void)r;
   return s.bytes();
 }
@@ -237,8 +312,8 @@ extern "C" inch_status inch_spmm(int32_t prec, int64_t n_atoms, const int64_t* r
   double *partial = nullptr, *coef = nullptr;
   if (e.r > 0) {
     Carver c(ws, ws_bytes);
-    partial = c.take<double>((size_t)kQxBlocks * 8 * 16);
-    coef = c.take<double>(8 * 16);
+    partial = c.take<double>((size_t)kQxBlocks * 8 * 64);
+    coef = c.take<double>(8 * 64);
     INCH_REQUIRE(c.ok, INCH_OOM, "inch_spmm: workspace of %zu bytes, need %zu", ws_bytes,
                  inch_spmm_workspace_size(n_atoms, b, e.r));
   }

@@ -14,6 +14,36 @@ import torch
 
 from . import _native, graph
 
+# Optional recorder of SpMM calls (CUDA events + algorithmic bytes); set by
+# measurement code, None otherwise.
+_probe = None
+
+
+class SpmmProbe:
+    """Records, for every store product issued while active, start/end CUDA events
+    on the launching (current) stream and the call's algorithmic bytes:
+    store once + X read once + Y written once (+ Yin / Acc traffic)."""
+
+    def __init__(self, prec=None):
+        self.prec = prec
+        self.records = []
+
+    def __enter__(self):
+        global _probe
+        _probe = self
+        return self
+
+    def __exit__(self, *a):
+        global _probe
+        _probe = None
+
+    def summary(self):
+        torch.cuda.synchronize()
+        ms = sum(s.elapsed_time(e) for s, e, _, _ in self.records)
+        nbytes = sum(b for _, _, b, _ in self.records)
+        calls = len(self.records)
+        return dict(calls=calls, ms=ms, bytes=nbytes, launches=sum(l for *_, l in self.records))
+
 
 class HessianStore:
     """ANM Hessian H + PlusI*I of a structure whose atoms are already in the
@@ -77,7 +107,33 @@ class HessianStore:
         if out is None:
             out = torch.empty_like(X)
         ent, diag = self.store(prec)
-        return _native.spmm(prec, self.n_atoms, self.rowptr, ent, diag, X, out, **epilogue)
+        probe = _probe if (_probe is not None and (_probe.prec is None or _probe.prec == prec)) else None
+        if probe is not None:
+            b = 1 if X.dim() == 1 else X.shape[1]
+            vec = X.element_size() * X.shape[0] * b
+            nbytes = self.store_bytes(prec) + vec * (2 + (epilogue.get("Yin") is not None)
+                                                     + 2 * (epilogue.get("acc") is not None))
+            ev0 = torch.cuda.Event(enable_timing=True)
+            ev1 = torch.cuda.Event(enable_timing=True)
+            ev0.record()
+            out = self._matmul(prec, ent, diag, X, out, epilogue)
+            ev1.record()
+            probe.records.append((ev0, ev1, nbytes, _launches(b, prec)))
+            return out
+        return self._matmul(prec, ent, diag, X, out, epilogue)
+
+    def _matmul(self, prec, ent, diag, X, out, epilogue):
+        if X.dim() == 1 or X.shape[1] <= 64:
+            return _native.spmm(prec, self.n_atoms, self.rowptr, ent, diag, X, out, **epilogue)
+        # the kernel takes up to 64 columns per call: walk column panels
+        for c0 in range(0, X.shape[1], 64):
+            sl = slice(c0, min(c0 + 64, X.shape[1]))
+            kw = dict(epilogue)
+            for key in ("Yin", "acc"):
+                if kw.get(key) is not None:
+                    kw[key] = kw[key][:, sl]
+            _native.spmm(prec, self.n_atoms, self.rowptr, ent, diag, X[:, sl], out[:, sl], **kw)
+        return out
 
     def __matmul__(self, X):
         return self.matmul(X)
@@ -111,3 +167,16 @@ class HessianStore:
         A = sp.csr_matrix((V[keep], (R[keep], C[keep])), shape=self.shape)
         A.sum_duplicates()
         return A
+
+
+def _launches(b, prec):
+    """SpMM kernel launches for b columns (tiles of 64/32/16/8/4/2/1 in FP32,
+    32/16/8/4/2/1 in FP64, per 64-column panel)."""
+    n = 0
+    for c0 in range(0, b, 64):
+        rem = min(64, b - c0)
+        for t in ((64, 32, 16, 8, 4, 2, 1) if prec == 32 else (32, 16, 8, 4, 2, 1)):
+            while rem >= t:
+                rem -= t
+                n += 1
+    return n

@@ -1,0 +1,191 @@
+"""Block Chebyshev-filtered subspace iteration with locking and explicit deflation
+(the many-mode solver of this package; no single reference function).
+
+It computes the same quantity as the reference's filtered TRLM ("CTRLM",
+InchingLiteInteger/Burn/ThickRestartLanczosHotellingDeflation/T1.py with
+User_PolynomialParams, driven window by window in
+Notebook/Application/04_Inching_EigenproblemManyCTRLM.ipynb): the lowest k
+non-rigid modes of H + PlusI*I.  Instead of one vector at a time it filters a
+whole block, so every Hessian application is a multivector SpMM and every
+projection a tall-skinny GEMM:
+
+  Y <- p_m(H) Y        scaled Chebyshev filter damping [a, b] (a = largest Ritz
+                       value of the block, b = spectrum upper bound), one fused
+                       SpMM per degree (Zhou & Saad, J. Comput. Phys. 219 (2006),
+                       Alg. "Chebyshev filter with scaling")
+  Y <- Y - Q Q^T Y     explicit deflation of the rigid-body basis and of locked
+                       modes (FP64 GEMMs)
+  Y <- orth(Y)         Cholesky-QR twice (FP64)
+  Rayleigh-Ritz        G = Y^T H Y, eigh (FP64), rotate; residuals ||H y - theta y||
+  lock                 leading Ritz pairs with residual <= tol * ||H||
+
+precision="mixed": filter and in-loop Rayleigh-Ritz products on the FP32 store
+with FP32 blocks; projections, orthonormalisation, the small eigenproblems and
+a final FP64 Rayleigh-Ritz + residual pass over the locked modes in FP64.
+precision="f64": everything FP64.
+"""
+from __future__ import annotations
+
+import math
+import time
+
+import numpy as np
+import torch
+
+from ..krylov import HessianOperator
+from ..spectrum import estimate_spectrum_bound
+
+
+def _cholqr(Y):
+    """Orthonormalise columns of Y (FP64) by Cholesky-QR applied twice."""
+    for _ in range(2):
+        G = Y.t() @ Y
+        try:
+            R = torch.linalg.cholesky(G, upper=True)
+        except RuntimeError:
+            Qf, _ = torch.linalg.qr(Y)
+            return Qf
+        Y = torch.linalg.solve_triangular(R, Y, upper=True, left=False)
+    return Y
+
+
+def _project_out(Y, B):
+    """Y <- Y - B^T (B Y) for row-basis B (r, n), twice."""
+    if B is None or B.shape[0] == 0:
+        return Y
+    for _ in range(2):
+        Y = Y - B.t() @ (B @ Y)
+    return Y
+
+
+class _Filter:
+    def __init__(self, A, prec):
+        self.A = A
+        self.prec = prec
+        self.n_spmm = 0
+
+    def __call__(self, X64, m, a, b, a0):
+        """Scaled Chebyshev filter of degree m on [a, b] normalised at a0 < a."""
+        dt = torch.float64 if self.prec == 64 else torch.float32
+        e = (b - a) / 2.0
+        c = (b + a) / 2.0
+        sigma = e / (a0 - c)
+        sigma1 = sigma
+        tau = 2.0 / sigma1
+        X = X64.to(dt).clone()         # the recurrence overwrites X
+        Y = torch.empty_like(X)
+        self.A.matmul(X, out=Y, prec=self.prec, alpha=sigma1 / e, gamma=-sigma1 * c / e)
+        self.n_spmm += 1
+        for _ in range(2, m + 1):
+            s2 = 1.0 / (tau - sigma)
+            # X <- 2 s2/e (H Y - c Y) - sigma s2 X, written over X, then swap
+            self.A.matmul(Y, out=X, prec=self.prec, alpha=2.0 * s2 / e, gamma=-2.0 * s2 * c / e,
+                          beta=-sigma * s2, Yin=X)
+            X, Y = Y, X
+            sigma = s2
+            self.n_spmm += 1
+        return Y.to(torch.float64)
+
+
+def _rr(A, Y, prec):
+    """Rayleigh-Ritz on orthonormal Y (n, p): returns theta (asc, numpy), Y W, (H Y) W."""
+    if prec == 64:
+        HY = A.matmul(Y.contiguous(), prec=64)
+    else:
+        HY = A.matmul(Y.to(torch.float32).contiguous(), prec=32).to(torch.float64)
+    G = Y.t() @ HY
+    G = 0.5 * (G + G.t())
+    th, W = np.linalg.eigh(G.cpu().numpy())
+    Wd = torch.from_numpy(W).to(Y.device)
+    return th, Y @ Wd, HY @ Wd
+
+
+def chfsi(A, k, tol=1e-6, Q=None, precision="mixed", degree=24, guard=None, maxiter=300, X0=None, seed=0,
+          spectrum_upper=None, final_f64=True, verbose=False, return_info=False):
+    """Lowest k eigenpairs of A (+PlusI) orthogonal to the rows of Q.
+
+    tol is relative: a pair is locked when ||H y - theta y|| <= tol * ||H||, with
+    ||H|| estimated by the Lanczos upper bound of the spectrum.
+    Returns (eigenvalues (k,) ascending, eigenvectors (n, k)) as FP64 CUDA tensors."""
+    t_start = time.perf_counter()
+    n = A.shape[0]
+    dev = A.device
+    assert 0 < k < n, "ABORTED. k must be in (0, n)"
+    assert precision in ("f64", "mixed"), "ABORTED. precision must be 'f64' or 'mixed'"
+    prec = 32 if precision == "mixed" else 64
+    if guard is None:
+        guard = max(16, int(math.ceil(0.15 * k)))
+    p = min(k + guard, n - (0 if Q is None else Q.shape[0]))
+    Qd = None if Q is None else HessianOperator(A, Q=Q).Q
+    if spectrum_upper is None:
+        lo, hi = estimate_spectrum_bound(A, steps=40, seed=seed + 1, precision=precision)
+        spectrum_upper = hi * 1.02 + 1e-3 * abs(hi)
+    b_up = float(spectrum_upper)
+    normH = b_up
+    g = torch.Generator(device=dev)
+    g.manual_seed(seed)
+    Y = torch.randn((n, p), generator=g, dtype=torch.float64, device=dev)
+    if X0 is not None:
+        X0 = X0.to(device=dev, dtype=torch.float64)
+        c0 = min(X0.shape[1], p)
+        Y[:, :c0] = X0[:, :c0]
+    Y = _cholqr(_project_out(Y, Qd))
+    th, Y, HY = _rr(A, Y, prec)
+    filt = _Filter(A, prec)
+    locked = torch.empty((0, n), dtype=torch.float64, device=dev)   # rows
+    locked_theta = []
+    it = 0
+    n_rr = 1
+    res = np.full(p, np.inf)
+    for it in range(maxiter):
+        R = HY - Y * torch.from_numpy(th).to(dev)[None, :]
+        res = torch.linalg.vector_norm(R, dim=0).cpu().numpy()
+        want = k - locked.shape[0]
+        nl = 0
+        while nl < min(want, Y.shape[1]) and res[nl] <= tol * normH:
+            nl += 1
+        if nl:
+            locked = torch.cat([locked, Y[:, :nl].t()], dim=0)
+            locked_theta.extend(th[:nl].tolist())
+            Y, HY, th = Y[:, nl:], HY[:, nl:], th[nl:]
+        if verbose:
+            print(f"it {it} locked {locked.shape[0]}/{k} maxres(active wanted) "
+                  f"{res[nl:want].max() / normH if want > nl else 0:.2e} a={th[-1]:.4f}")
+        if locked.shape[0] >= k:
+            break
+        a = float(th[-1])
+        a0 = float(min(th[0], locked_theta[0] if locked_theta else th[0]))
+        if not (a0 < a < b_up):
+            a0 = a - 1e-3 * abs(a)
+        Z = filt(Y, degree, a, b_up, a0 - 1e-12)
+        Z = _project_out(Z, Qd)
+        Z = _project_out(Z, locked)
+        Z = _cholqr(Z)
+        th, Y, HY = _rr(A, Z, prec)
+        n_rr += 1
+    converged = locked.shape[0] >= k
+    if not converged:
+        print(f"ABORTED. chfsi did not converge in {maxiter} iterations: {locked.shape[0]} of {k} modes locked")
+        extra = k - locked.shape[0]
+        locked = torch.cat([locked, Y[:, :extra].t()], dim=0)
+        locked_theta.extend(th[:extra].tolist())
+    L = locked[:k].t().contiguous()
+    if final_f64:
+        th_f, L, HL = _rr(A, L, 64)
+        R = HL - L * torch.from_numpy(th_f).to(dev)[None, :]
+        final_res = torch.linalg.vector_norm(R, dim=0).cpu().numpy() / normH
+        evals = th_f
+    else:
+        evals = np.asarray(locked_theta[:k])
+        idx = np.argsort(evals)
+        evals = evals[idx]
+        L = L[:, torch.from_numpy(idx).to(dev)]
+        final_res = None
+    evals_t = torch.from_numpy(np.ascontiguousarray(evals)).to(dev)
+    if return_info:
+        info = dict(iterations=it + 1, converged=converged, n_spmm_filter=filt.n_spmm, n_rr=n_rr,
+                    normH=normH, degree=degree, block=p,
+                    max_rel_residual=None if final_res is None else float(final_res.max()),
+                    seconds=time.perf_counter() - t_start)
+        return evals_t, L, info
+    return evals_t, L

@@ -193,8 +193,11 @@ def gmres_deflate(matvec, b, x0, uu, tol, restart=20, maxiter=20):
 
 
 def jdm(op, n, k=16, tol=1e-10, maxiter=1000, correction_maxiter=20, workspace_factor=2,
-        intermediate_tol=1e-3, gap=0.1, factoring_tol=1e-4, Q=None, shift=10.0, seed=0):
-    """Returns (eigenvalues ascending, eigenvectors (n, k), iterations, converged)."""
+        intermediate_tol=1e-3, gap=0.1, factoring_tol=1e-4, Q=None, shift=10.0, seed=0, time_budget=None):
+    """Returns (eigenvalues ascending, eigenvectors (n, k), iterations, converged).
+    With time_budget (s) the iteration stops early and returns what it has."""
+    import time as _time
+    t_start = _time.perf_counter()
     rng = np.random.default_rng(seed)
     jmax = k * workspace_factor
     jmin = min(n, k)
@@ -212,6 +215,9 @@ def jdm(op, n, k=16, tol=1e-10, maxiter=1000, correction_maxiter=20, workspace_f
     jacc = 0
     jcur = 1
     for it in range(maxiter):
+        if time_budget is not None and _time.perf_counter() - t_start > time_budget:
+            idx = np.argsort(eig[:max(nconv, 1)])
+            return eig[idx], Qc[:, idx], it, False
         S, W = np.linalg.eigh(G, UPLO="L")
         while True:
             theta = S[0]

@@ -1,0 +1,168 @@
+"""GPU eigensolvers against the FP64 oracle (dense LAPACK on the oracle Hessian)
+and the reference-algorithm restatements.
+
+Tolerances (stated per the metric): eigenvalues relative 1e-9 for the FP64
+solvers at tight tolerance; mixed precision at residual 1e-6*||H|| -> relative
+eigenvalue error <= 1e-6 and largest principal angle per degenerate cluster
+<= 1e-2 rad; FP64 at 1e-9*||H|| -> angle <= 1e-5 rad."""
+import numpy as np
+import pytest
+import torch
+
+from oracle import hessian as oh
+from oracle import solvers as osv
+
+pytestmark = pytest.mark.gpu
+
+
+@pytest.fixture(scope="module")
+def small():
+    from inching_b200 import graph, synth
+    from inching_b200.deflation import rigid_body_basis
+    from inching_b200.hessian import HessianStore
+    X = synth.globule(1200, seed=9) / 10.0
+    order, _ = graph.cuthill_mckee(X, 8.0)
+    Xr = X[order.cpu().numpy()]
+    H = HessianStore(Xr, 8.0, plus_i=1.0)
+    A, Ad = oh.hessian_lower(Xr, 8.0, 1.0)
+    Hd = oh.full_from_lower(A, Ad).toarray()
+    w, U = np.linalg.eigh(Hd)
+    Q = rigid_body_basis(torch.from_numpy(Xr).cuda())
+    return dict(Xr=Xr, H=H, A=A, Ad=Ad, Hd=Hd, w=w, U=U, Q=Q)
+
+
+def max_cluster_angle(V, U, w, lo, hi, gap_tol=1e-6):
+    """Largest principal angle between span(V) and the exact eigenspace of
+    eigenvalues w[lo:hi], taken over clusters of (near-)degenerate eigenvalues."""
+    Vo, _ = np.linalg.qr(V)
+    s = np.linalg.svd(U[:, lo:hi].T @ Vo, compute_uv=False)
+    return float(np.arccos(np.clip(s.min(), -1, 1)))
+
+
+def test_trlm_f64_matches_dense(small):
+    from inching_b200.Burn.ThickRestartLanczosHotellingDeflation.T1 import S_HeigvalTRLMHD_HeigvecTRLMHD
+    s = small
+    S, V = S_HeigvalTRLMHD_HeigvecTRLMHD(s["H"], s["H"].A_diag, k=24, tol=1e-9, User_Q_HotellingDeflation=s["Q"],
+                                        User_HotellingShift=10.0)
+    ref = s["w"][6:30]
+    assert np.max(np.abs(S.cpu().numpy() - ref) / ref) < 1e-9
+    V = V.cpu().numpy()
+    assert V.shape == (s["H"].shape[0], 24)
+    res = np.linalg.norm(s["Hd"] @ V - V * S.cpu().numpy()[None, :], axis=0)
+    assert res.max() < 1e-7
+    assert max_cluster_angle(V, s["U"], s["w"], 6, 30) < 1e-3
+
+
+def test_trlm_mixed_precision(small):
+    from inching_b200.solvers.trlm import trlm
+    s = small
+    S, V = trlm(s["H"], k=16, tol=1e-6, Q=s["Q"], shift=10.0, precision="mixed")
+    assert np.max(np.abs(S.cpu().numpy() - s["w"][6:22]) / s["w"][6:22]) < 1e-6
+
+
+def test_jdm_matches_dense(small):
+    from inching_b200.Burn.JacobiDavidsonHotellingDeflation.T1 import S_HeigvalJDMHD_HeigvecJDMHD
+    s = small
+    S, V = S_HeigvalJDMHD_HeigvecJDMHD(s["H"], s["H"].A_diag, k=12, tol=1e-9, User_Q_HotellingDeflation=s["Q"],
+                                      User_HotellingShift=10.0)
+    ref = s["w"][6:18]
+    assert np.max(np.abs(S.cpu().numpy() - ref) / ref) < 1e-9
+    res = np.linalg.norm(s["Hd"] @ V.cpu().numpy() - V.cpu().numpy() * S.cpu().numpy()[None, :], axis=0)
+    assert res.max() < 1e-8
+
+
+def test_jdm_agrees_with_oracle_restatement(small):
+    """Same algorithm on CPU (oracle) and GPU: same eigenvalues."""
+    from inching_b200.solvers.jdm import jdm
+    s = small
+    op = lambda v: oh.krylov_av(s["A"], s["Ad"], v)
+    Qn = s["Q"].cpu().numpy()
+    So, Vo, _, conv = osv.jdm(op, s["H"].shape[0], k=8, tol=1e-9, Q=Qn, shift=10.0)
+    Sg, Vg = jdm(s["H"], k=8, tol=1e-9, Q=s["Q"], shift=10.0)
+    assert conv and np.max(np.abs(Sg.cpu().numpy() - So)) < 1e-9
+
+
+def test_irlm_matches_dense(small):
+    from inching_b200.Burn.ImplicitlyRestartedLanczosHotellingDeflation.T1 import S_HeigvalIRLMHD_HeigvecIRLMHD
+    s = small
+    S, V = S_HeigvalIRLMHD_HeigvecIRLMHD(s["H"], k=32, tol=1e-9, User_Q_HotellingDeflation=s["Q"],
+                                        User_HotellingShift=10.0)
+    ref = s["w"][6:38]
+    assert np.max(np.abs(S.cpu().numpy() - ref) / ref) < 1e-8
+
+
+@pytest.mark.parametrize("precision,tol,eig_tol,ang_tol", [("f64", 1e-9, 1e-10, 1e-5), ("mixed", 1e-6, 1e-6, 1e-2)])
+def test_chfsi_matches_dense(small, precision, tol, eig_tol, ang_tol):
+    from inching_b200.solvers.chfsi import chfsi
+    s = small
+    S, V, info = chfsi(s["H"], 60, tol=tol, Q=s["Q"], precision=precision, return_info=True)
+    ref = s["w"][6:66]
+    assert info["converged"]
+    assert np.max(np.abs(S.cpu().numpy() - ref) / ref) < eig_tol
+    assert info["max_rel_residual"] <= tol * 1.5
+    assert max_cluster_angle(V.cpu().numpy(), s["U"], s["w"], 6, 66) < ang_tol
+
+
+def test_chebyshev_filter_matches_oracle(small):
+    from inching_b200 import polyfilter
+    from inching_b200.krylov import ChebyshevFilter
+    s = small
+    pol = polyfilter.OOC0_OptimizePolynomialParamsOnDegree(User_WantedInterval=(1.0, 3.0),
+                                                           User_SpectrumBound=(0.99, s["w"][-1] * 1.01),
+                                                           User_MaximumDegree=300)
+    v = np.random.default_rng(1).standard_normal(s["H"].shape[0])
+    op = lambda x: oh.krylov_av(s["A"], s["Ad"], x)
+    ref = osv.chebyshev_av(op, v, pol.AdjustedCoefficients, pol.cc, pol.dd, pol.AdjustedDegree)
+    for prec, tol in ((64, 1e-10), (32, 1e-4)):
+        y = ChebyshevFilter(s["H"], pol, prec=prec)(torch.from_numpy(v).cuda()).double().cpu().numpy()
+        assert np.abs(y - ref).max() <= tol * np.abs(ref).max()
+
+
+def test_filtered_trlm_and_spectrum_bound(small):
+    from inching_b200 import polyfilter
+    from inching_b200.Burn.HermitianLanczos.T2 import A_Adiag_EstimateSpectrumBound
+    from inching_b200.solvers.trlm import trlm
+    s = small
+    lo, hi = A_Adiag_EstimateSpectrumBound(s["H"], s["H"].A_diag)
+    assert abs(hi - s["w"][-1]) < 1e-6 * s["w"][-1] and abs(lo - s["w"][0]) < 1e-6
+    pol = polyfilter.OOC0_OptimizePolynomialParamsOnDegree(User_WantedInterval=(1.0, s["w"][20]),
+                                                           User_SpectrumBound=(lo, hi), User_MaximumDegree=600,
+                                                           User_ConvergenceRatio=0.7)
+    S, V = trlm(s["H"], k=8, tol=1e-8, Q=s["Q"], shift=-40.0, polynomial=pol)
+    assert np.max(np.abs(S.cpu().numpy() - s["w"][6:14]) / s["w"][6:14]) < 1e-8
+
+
+def test_kpm_count_brackets_true_count(small):
+    from inching_b200 import polyfilter
+    from inching_b200.spectrum import kpm_count
+    s = small
+    w = s["w"]
+    lo, hi = 0.5 * (w[9] + w[10]), 0.5 * (w[80] + w[81])
+    pol = polyfilter.OOC0_OptimizePolynomialParamsOnDegree(User_WantedInterval=(lo, hi),
+                                                           User_SpectrumBound=(w[0] - 1e-3, w[-1] * 1.01),
+                                                           User_MaximumDegree=3000)
+    true = int(np.sum((w >= lo) & (w <= hi)))
+    est = kpm_count(s["H"], pol, trials=400)
+    assert abs(est - true) <= 0.3 * true
+
+
+def test_pipeline_undo_order_and_rigid_orthogonality():
+    """Host API: modes come back in the caller's atom order, orthogonal to the
+    rigid-body motions, eigenvalues with PlusI removed (driver layout)."""
+    from inching_b200 import synth
+    from inching_b200.pipeline import normal_modes
+    X = synth.globule(900, seed=12) / 10.0
+    perm = np.random.default_rng(0).permutation(900)
+    ev, modes, info = normal_modes(X, 20, solver="chfsi", precision="f64", tol=1e-9)
+    ev2, modes2, _ = normal_modes(X[perm], 20, solver="chfsi", precision="f64", tol=1e-9)
+    assert modes.shape == (20, 900, 3)
+    assert np.allclose(ev, ev2, rtol=1e-8, atol=1e-10)
+    A, Ad = oh.hessian_lower(X, 8.0, 1.0)
+    w = np.linalg.eigvalsh(oh.full_from_lower(A, Ad).toarray())
+    assert np.allclose(ev, w[6:26] - 1.0, rtol=1e-8, atol=1e-10)
+    Q = oh.rigid_body_basis(X)
+    assert np.abs(Q @ modes.reshape(20, -1).T).max() < 1e-8
+    # eigenvector of mode 0 of the permuted input maps back to the same atoms
+    v1 = modes[0].ravel()
+    v2 = modes2[0][np.argsort(perm)].ravel()
+    assert abs(abs(v1 @ v2) - 1.0) < 1e-6
