@@ -69,6 +69,9 @@ _SIGS = {
     "inch_spmm": (ctypes.c_int, [c_int32, c_int64, c_void_p, c_void_p, c_void_p, c_void_p, c_int64, c_int32,
                                  c_void_p, c_int64, c_void_p, c_int64, c_void_p, c_int64, c_void_p,
                                  POINTER(SpmmEpilogue), c_void_p, c_size_t, c_void_p]),
+    "inch_spmm_noalloc": (ctypes.c_int, [c_int32, c_int64, c_void_p, c_void_p, c_void_p, c_void_p, c_int64,
+                                         c_int32, c_void_p, c_int64, c_void_p, c_int64, c_void_p, c_int64,
+                                         c_void_p, POINTER(SpmmEpilogue), c_void_p]),
 }
 
 

@@ -328,3 +328,83 @@ extern "C" inch_status inch_spmm(int32_t prec, int64_t n_atoms, const int64_t* r
   INCH_REQUIRE(err == cudaSuccess, INCH_CUDA_ERROR, "inch_spmm: %s", cudaGetErrorString(err));
   return INCH_OK;
 }
+
+// ---------------------------------------------------------------------------
+// Allocation-free variant of inch_spmm.
+//
+// Some hosts cannot hand this library a device workspace: a caller that sits on
+// top of another runtime's memory manager with no device allocator of its own,
+// or a bare FFI binding that only owns its input and output buffers.  For them
+// the Hotelling partial sums and coefficients live in the file-scope array
+// below.  It is sized for the largest tile the kernels use (64 columns) and the
+// largest fused deflation rank (8): kQxBlocks * 8 * 64 + 8 * 64 doubles, about
+// 1.2 MB, resident on every GPU that loads the library until the process exits.
+// The array's host-side name is not a device address: its address is fetched
+// with cudaGetSymbolAddress once per device, with that device current, on the
+// first call made on that device (so make that first call before any stream
+// capture).  Nothing in the array has to start at zero: every call writes each
+// partial sum and coefficient before reading it.  All calls share the array, so
+// calls that overlap on the GPU (different streams, or different host threads on
+// the same device) race on it and must be serialised by the caller.
+// ---------------------------------------------------------------------------
+#include <mutex>
+
+namespace inch {
+namespace {
+constexpr size_t kNoAllocPartial = (size_t)kQxBlocks * 8 * 64;
+constexpr size_t kNoAllocDoubles = kNoAllocPartial + 8 * 64;
+constexpr int kNoAllocMaxDevices = 64;
+static __device__ __align__(256) double g_noalloc_scratch[kNoAllocDoubles];
+std::mutex g_noalloc_mu;
+double* g_noalloc_addr[kNoAllocMaxDevices] = {nullptr};
+}  // namespace
+}  // namespace inch
+
+extern "C" inch_status inch_spmm_noalloc(int32_t prec, int64_t n_atoms, const int64_t* rowptr, const void* ent,
+                                         const void* diag, const void* X, int64_t ldx, int32_t b, void* Y,
+                                         int64_t ldy, const void* Yin, int64_t ldyin, void* Acc, int64_t ldacc,
+                                         const double* q, const inch_spmm_epilogue* ep_in, cudaStream_t stream) {
+  INCH_REQUIRE(prec == 32 || prec == 64, INCH_INVALID_ARG, "inch_spmm_noalloc: prec must be 32 or 64");
+  INCH_REQUIRE(rowptr && ent && diag && X && Y && ep_in, INCH_INVALID_ARG, "inch_spmm_noalloc: NULL argument");
+  INCH_REQUIRE(n_atoms >= 1 && n_atoms < (int64_t(1) << 31), INCH_INVALID_ARG,
+               "inch_spmm_noalloc: n_atoms out of range");
+  INCH_REQUIRE(b >= 1 && b <= 64, INCH_LIMIT,
+               "inch_spmm_noalloc: b=%d exceeds the 64 columns its static scratch holds", b);
+  INCH_REQUIRE(ldx >= b && ldy >= b, INCH_INVALID_ARG, "inch_spmm_noalloc: leading dimension below b");
+  INCH_REQUIRE(X != Y, INCH_INVALID_ARG, "inch_spmm_noalloc: X and Y must not alias");
+  const inch_spmm_epilogue& e = *ep_in;
+  INCH_REQUIRE(e.r >= 0 && e.r <= 8, INCH_LIMIT,
+               "inch_spmm_noalloc: deflation rank %d exceeds the 8 its static scratch holds", e.r);
+  INCH_REQUIRE(e.r == 0 || q != nullptr, INCH_INVALID_ARG, "inch_spmm_noalloc: deflation basis is NULL");
+  INCH_REQUIRE(e.beta == 0.0 || (Yin != nullptr && ldyin >= b), INCH_INVALID_ARG,
+               "inch_spmm_noalloc: beta != 0 needs Yin");
+  INCH_REQUIRE(!e.accumulate || (Acc != nullptr && ldacc >= b), INCH_INVALID_ARG,
+               "inch_spmm_noalloc: accumulate needs Acc");
+  INCH_REQUIRE(((uintptr_t)ent & 15) == 0 && ((uintptr_t)diag & 15) == 0, INCH_INVALID_ARG,
+               "inch_spmm_noalloc: store buffers must be 16-byte aligned");
+  int dev = -1;
+  INCH_CUDA(cudaGetDevice(&dev));
+  INCH_REQUIRE(dev >= 0 && dev < kNoAllocMaxDevices, INCH_LIMIT, "inch_spmm_noalloc: device %d not supported", dev);
+  double* base = nullptr;
+  {
+    std::lock_guard<std::mutex> lock(g_noalloc_mu);
+    if (g_noalloc_addr[dev] == nullptr) {
+      void* p = nullptr;
+      INCH_CUDA(cudaGetSymbolAddress(&p, g_noalloc_scratch));
+      g_noalloc_addr[dev] = static_cast<double*>(p);
+    }
+    base = g_noalloc_addr[dev];
+  }
+  double* partial = base;
+  double* coef = base + kNoAllocPartial;
+  Epi ep{e.alpha, e.gamma, e.beta, e.mu, e.r, e.accumulate, (e.beta != 0.0) ? 1 : 0};
+  cudaError_t err;
+  if (prec == 32)
+    err = run<float>(n_atoms, rowptr, ent, diag, X, ldx, b, Y, ldy, Yin, ldyin, Acc, ldacc, ep, q, e.hot_shift,
+                     partial, coef, stream);
+  else
+    err = run<double>(n_atoms, rowptr, ent, diag, X, ldx, b, Y, ldy, Yin, ldyin, Acc, ldacc, ep, q, e.hot_shift,
+                      partial, coef, stream);
+  INCH_REQUIRE(err == cudaSuccess, INCH_CUDA_ERROR, "inch_spmm_noalloc: %s", cudaGetErrorString(err));
+  return INCH_OK;
+}

@@ -166,6 +166,23 @@ inch_status inch_spmm(int32_t prec, int64_t n_atoms, const int64_t* rowptr_dev,
                       const inch_spmm_epilogue* ep,
                       void* ws_dev, size_t ws_bytes, cudaStream_t stream);
 
+/* Allocation-free form of inch_spmm (no counterpart in the reference).  For
+ * callers that cannot provide device scratch -- hosts running on another
+ * runtime's memory manager without a device allocator of their own, or thin FFI
+ * bindings that own only their input and output buffers -- the deflation partial
+ * sums live in a static device array of about 1.2 MB held by every GPU that
+ * loads the library until exit.  Limits: b <= 64 columns and r <= 8 deflation
+ * vectors (else INCH_LIMIT).  The first call on a device looks up the array's
+ * device address (cudaGetSymbolAddress); make that first call before any stream
+ * capture.  All calls share the array: calls that overlap on the GPU race and
+ * must be serialised by the caller.  Allocates nothing. */
+inch_status inch_spmm_noalloc(int32_t prec, int64_t n_atoms, const int64_t* rowptr_dev,
+                              const void* ent_dev, const void* diag_dev,
+                              const void* X_dev, int64_t ldx, int32_t b,
+                              void* Y_dev, int64_t ldy, const void* Yin_dev, int64_t ldyin,
+                              void* Acc_dev, int64_t ldacc, const double* q_dev,
+                              const inch_spmm_epilogue* ep, cudaStream_t stream);
+
 #ifdef __cplusplus
 }
 #endif
