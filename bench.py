@@ -35,6 +35,8 @@ ROOT = os.path.dirname(os.path.abspath(__file__))
 sys.path.insert(0, ROOT)
 
 METRIC = "time-to-k-modes (s) at resid <=1e-6||H||"
+TRAFFIC_B64_BYTES = 311_794_176
+TRAFFIC_B64_RATIO = 0.979
 UNIT = "s"
 
 
@@ -50,7 +52,41 @@ def parse():
     ap.add_argument("--no-plain", action="store_true", help="skip the plain FP64 JDM comparison")
     ap.add_argument("--no-cpu", action="store_true", help="skip the CPU baseline leg")
     ap.add_argument("--cpu-budget", type=float, default=15.0)
+    ap.add_argument("--kernel-only", default=None, choices=["spmm32", "spmm64"],
+                    help="profiling aid: build the workload's store and run only the SpMM")
+    ap.add_argument("--b", type=int, default=64, help="columns for --kernel-only")
+    ap.add_argument("--reps", type=int, default=5, help="launches for --kernel-only")
     return ap.parse_args()
+
+
+def run_kernel_only(args):
+    """Builds the workload's Hessian store and issues --reps SpMM calls on a
+    (3N, b) block; prints per-call CUDA-event time and algorithmic GB/s.  Used
+    to profile the dominant kernel in isolation (small, self-terminating)."""
+    import torch
+    from inching_b200 import graph, synth
+    from inching_b200.hessian import HessianStore
+    Xd = torch.from_numpy(synth.workload(args.workload) / 10.0).cuda()
+    order, _ = graph.cuthill_mckee(Xd, 8.0)
+    prec = 32 if args.kernel_only == "spmm32" else 64
+    H = HessianStore(Xd[order], 8.0, 1.0, precisions=("f32",) if prec == 32 else ("f64",))
+    dt = torch.float32 if prec == 32 else torch.float64
+    g = torch.Generator(device="cuda")
+    g.manual_seed(0)
+    X = torch.randn((H.shape[0], args.b), generator=g, dtype=torch.float64, device="cuda").to(dt).contiguous()
+    Y = torch.empty_like(X)
+    ev = [(torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)) for _ in range(args.reps)]
+    for e0, e1 in ev:
+        e0.record()
+        H.matmul(X, out=Y, prec=prec)
+        e1.record()
+    torch.cuda.synchronize()
+    ms = [e0.elapsed_time(e1) for e0, e1 in ev]
+    nbytes = H.store_bytes(prec) + 2 * X.numel() * X.element_size()
+    best = min(ms)
+    print(json.dumps({"kernel": args.kernel_only, "b": args.b, "n_atoms": H.n_atoms, "nnz": H.nnz_blocks,
+                      "ms": [round(m, 4) for m in ms], "algorithmic_bytes": nbytes,
+                      "best_GBps": round(nbytes / best / 1e6, 1)}))
 
 
 class Clocks:
@@ -266,7 +302,11 @@ def run_ours(args):
         "roofline": {"bound": "hbm", "achieved": round(achieved, 1) if achieved else None, "peak": hbm,
                      "unit": "GB/s", "frac": round(achieved / hbm, 4) if achieved else None,
                      "peak_kind": peak_kind, "kernel": "FP32 SpMM (k_spmm_cols / k_spmm)",
-                     "spmm_calls": sp["calls"], "spmm_ms": round(sp["ms"], 2), "traffic": None},
+                     "spmm_calls": sp["calls"], "spmm_ms": round(sp["ms"], 2),
+                     # ncu dram__bytes_read.sum + dram__bytes_write.sum of one 64-column FP32 launch on this
+                     # workload (profiles/spmm_f32_b64_assembly100k.md): 311.8 MB against 318.6 MB algorithmic
+                     "traffic": TRAFFIC_B64_BYTES, "traffic_unit": "bytes per 64-column launch",
+                     "traffic_over_algorithmic": TRAFFIC_B64_RATIO},
         "cpu_baseline": cpu,
         "clocks": clk.summary(),
         "gpu_launches": int(launches),
@@ -305,7 +345,9 @@ def run_reference(args):
 
 if __name__ == "__main__":
     a = parse()
-    if a.impl == "reference":
+    if a.kernel_only:
+        run_kernel_only(a)
+    elif a.impl == "reference":
         run_reference(a)
     else:
         run_ours(a)
