@@ -56,6 +56,8 @@ def parse():
                     help="profiling aid: build the workload's store and run only the SpMM")
     ap.add_argument("--b", type=int, default=64, help="columns for --kernel-only")
     ap.add_argument("--reps", type=int, default=5, help="launches for --kernel-only")
+    ap.add_argument("--tune", default=None, help="threads,blocks_per_sm for the wide SpMM (--kernel-only)")
+    ap.add_argument("--layout", default="tiles", choices=["tiles", "pairs"], help="store layout for --kernel-only")
     return ap.parse_args()
 
 
@@ -66,10 +68,15 @@ def run_kernel_only(args):
     import torch
     from inching_b200 import graph, synth
     from inching_b200.hessian import HessianStore
+    from inching_b200 import _native
+    if args.tune:
+        t, bps = (int(x) for x in args.tune.split(","))
+        _native.spmm_tune(t, bps)
     Xd = torch.from_numpy(synth.workload(args.workload) / 10.0).cuda()
     order, _ = graph.cuthill_mckee(Xd, 8.0)
     prec = 32 if args.kernel_only == "spmm32" else 64
-    H = HessianStore(Xd[order], 8.0, 1.0, precisions=("f32",) if prec == 32 else ("f64",))
+    H = HessianStore(Xd[order], 8.0, 1.0, precisions=("f32",) if prec == 32 else ("f64",),
+                     tiles=args.layout == "tiles")
     dt = torch.float32 if prec == 32 else torch.float64
     g = torch.Generator(device="cuda")
     g.manual_seed(0)
@@ -82,9 +89,9 @@ def run_kernel_only(args):
         e1.record()
     torch.cuda.synchronize()
     ms = [e0.elapsed_time(e1) for e0, e1 in ev]
-    nbytes = H.store_bytes(prec) + 2 * X.numel() * X.element_size()
+    nbytes = H.store_bytes(prec, args.b) + 2 * X.numel() * X.element_size()
     best = min(ms)
-    print(json.dumps({"kernel": args.kernel_only, "b": args.b, "n_atoms": H.n_atoms, "nnz": H.nnz_blocks,
+    print(json.dumps({"kernel": args.kernel_only, "b": args.b, "tune": args.tune, "layout": args.layout, "n_atoms": H.n_atoms, "nnz": H.nnz_blocks,
                       "ms": [round(m, 4) for m in ms], "algorithmic_bytes": nbytes,
                       "best_GBps": round(nbytes / best / 1e6, 1)}))
 

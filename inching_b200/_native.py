@@ -66,9 +66,19 @@ _SIGS = {
     "inch_hessian_assemble": (ctypes.c_int, [c_void_p, c_int64, c_double, c_double, c_void_p, c_void_p,
                                              c_void_p, c_void_p, c_void_p, c_void_p, c_void_p]),
     "inch_spmm_workspace_size": (c_size_t, [c_int64, c_int32, c_int32]),
+    "inch_spmm_tune": (ctypes.c_int, [c_int32, c_int32]),
     "inch_spmm": (ctypes.c_int, [c_int32, c_int64, c_void_p, c_void_p, c_void_p, c_void_p, c_int64, c_int32,
                                  c_void_p, c_int64, c_void_p, c_int64, c_void_p, c_int64, c_void_p,
                                  POINTER(SpmmEpilogue), c_void_p, c_size_t, c_void_p]),
+    "inch_tile_store_workspace_size": (c_size_t, [c_int64]),
+    "inch_tile_store_count": (ctypes.c_int, [c_void_p, c_void_p, c_int64, c_void_p, c_void_p, POINTER(c_int64),
+                                             POINTER(c_int64), c_void_p, c_size_t, c_void_p]),
+    "inch_tile_store_fill": (ctypes.c_int, [c_void_p, c_int64, c_double, c_void_p, c_void_p, c_void_p, c_void_p,
+                                            c_void_p, c_void_p, c_void_p, c_void_p]),
+    "inch_spmm_tiles_workspace_size": (c_size_t, []),
+    "inch_spmm_tiles": (ctypes.c_int, [c_int32, c_int64, c_void_p, c_void_p, c_void_p, c_void_p, c_void_p,
+                                       c_void_p, c_int64, c_int32, c_void_p, c_int64, c_void_p, c_int64, c_void_p,
+                                       c_int64, c_void_p, POINTER(SpmmEpilogue), c_void_p, c_size_t, c_void_p]),
     "inch_spmm_noalloc": (ctypes.c_int, [c_int32, c_int64, c_void_p, c_void_p, c_void_p, c_void_p, c_int64,
                                          c_int32, c_void_p, c_int64, c_void_p, c_int64, c_void_p, c_int64,
                                          c_void_p, POINTER(SpmmEpilogue), c_void_p]),
@@ -212,6 +222,11 @@ def hessian_assemble(X, rowptr, cols, rc_nm, plus_i, want64=True, want32=True):
 _ws_cache = {}
 
 
+def spmm_tune(threads_per_block=256, blocks_per_sm=5):
+    """Set the wide-block SpMM launch shape for this process (autotuner hook)."""
+    check(lib().inch_spmm_tune(threads_per_block, blocks_per_sm))
+
+
 def spmm(prec, n_atoms, rowptr, ent, diag, X, Y, *, alpha=1.0, gamma=0.0, beta=0.0, Yin=None,
          acc=None, mu=0.0, Q=None, hot_shift=0.0):
     """Y = alpha*(H X) + gamma*X + beta*Yin + hot_shift*Q^T(Q X); acc += mu*Y if acc given.
@@ -234,6 +249,62 @@ def spmm(prec, n_atoms, rowptr, ent, diag, X, Y, *, alpha=1.0, gamma=0.0, beta=0
     check(L.inch_spmm(prec, n_atoms, _ptr(rowptr), _ptr(ent), _ptr(diag), _ptr(X), ldx, b, _ptr(Y), ldy,
                       _ptr(Yin), ldyin, _ptr(acc), ldacc, _ptr(Q), ctypes.byref(ep), _ptr(ws), ws.numel(),
                       _stream()))
+    tiles = 0
+    rem = b
+    for t in ((64, 32, 16, 8, 4, 2, 1) if prec == 32 else (32, 16, 8, 4, 2, 1)):
+        while rem >= t:
+            rem -= t
+            tiles += 1
+    _count(tiles * (3 if r > 0 else 1))
+    return Y
+
+
+# ---------------------------------------------------------------------------
+# Row-tile store (wide multivectors)
+# ---------------------------------------------------------------------------
+def tile_store(X, rowptr, cols, rc_nm, want64=True, want32=True):
+    """(tile_uptr, tile_pptr, urec, pw64, pw32, n_union, n_pairs) for 8-row tiles."""
+    L = lib()
+    n = X.shape[0]
+    dev = X.device
+    nt = (n + 7) // 8
+    uptr = torch.empty(nt + 1, dtype=torch.int64, device=dev)
+    pptr = torch.empty(nt + 1, dtype=torch.int64, device=dev)
+    ws = _ws(L.inch_tile_store_workspace_size(n), dev)
+    nu, npairs = c_int64(0), c_int64(0)
+    check(L.inch_tile_store_count(_ptr(rowptr), _ptr(cols), n, _ptr(uptr), _ptr(pptr), ctypes.byref(nu),
+                                  ctypes.byref(npairs), _ptr(ws), ws.numel(), _stream()))
+    urec = torch.empty(max(nu.value, 1), dtype=torch.int32, device=dev)
+    pw64 = torch.empty((max(npairs.value, 1), 4), dtype=torch.float64, device=dev) if want64 else None
+    pw32 = torch.empty((max(npairs.value, 1), 4), dtype=torch.float32, device=dev) if want32 else None
+    check(L.inch_tile_store_fill(_ptr(X), n, rc_nm, _ptr(rowptr), _ptr(cols), _ptr(uptr), _ptr(pptr), _ptr(urec),
+                                 _ptr(pw64), _ptr(pw32), _stream()))
+    _count(4)
+    return uptr, pptr, urec, pw64, pw32, nu.value, npairs.value
+
+
+_tws = {}
+
+
+def spmm_tiles(prec, n_atoms, uptr, pptr, urec, pw, diag, X, Y, *, alpha=1.0, gamma=0.0, beta=0.0, Yin=None,
+               acc=None, mu=0.0, Q=None, hot_shift=0.0):
+    """Same contract as spmm(), on the row-tile store."""
+    L = lib()
+    b = 1 if X.dim() == 1 else X.shape[1]
+    ldx = 1 if X.dim() == 1 else X.stride(0)
+    ldy = 1 if Y.dim() == 1 else Y.stride(0)
+    ldyin = 0 if Yin is None else (1 if Yin.dim() == 1 else Yin.stride(0))
+    ldacc = 0 if acc is None else (1 if acc.dim() == 1 else acc.stride(0))
+    r = 0 if Q is None else Q.shape[0]
+    ep = SpmmEpilogue(alpha, gamma, beta, mu, hot_shift, r, 1 if acc is not None else 0)
+    dev = X.device
+    ws = _tws.get(dev.index)
+    if ws is None:
+        ws = _ws(L.inch_spmm_tiles_workspace_size(), dev)
+        _tws[dev.index] = ws
+    check(L.inch_spmm_tiles(prec, n_atoms, _ptr(uptr), _ptr(pptr), _ptr(urec), _ptr(pw), _ptr(diag), _ptr(X), ldx,
+                            b, _ptr(Y), ldy, _ptr(Yin), ldyin, _ptr(acc), ldacc, _ptr(Q), ctypes.byref(ep),
+                            _ptr(ws), ws.numel(), _stream()))
     tiles = 0
     rem = b
     for t in ((64, 32, 16, 8, 4, 2, 1) if prec == 32 else (32, 16, 8, 4, 2, 1)):

@@ -15,6 +15,8 @@
 // lanes of the group stride over the row's entries (one 16-byte load per entry in
 // FP32, two in FP64), gather X_j from L1/L2 (rows are banded after Cuthill-McKee
 // so neighbouring rows share their X_j), and reduce with xor shuffles.
+#include <atomic>
+
 #include "common.cuh"
 
 namespace inch {
@@ -51,6 +53,12 @@ struct Ent<double> {
 };
 
 constexpr int kThreads = 256;
+
+// Launch shape of the wide-block kernel (threads per block, blocks per SM):
+// process-wide, set by inch_spmm_tune (the autotuner's hook).
+std::atomic<int> g_cols_threads{256};
+std::atomic<int> g_cols_blocks_per_sm{5};
+std::atomic<int> g_warp_kernel{0};   // 1: whole-warp rows with batched gathers where B/V >= 32
 
 template <class T, int B, int G>
 __global__ void __launch_bounds__(kThreads)
@@ -117,36 +125,73 @@ k_spmm(int64_t n_atoms, const int64_t* __restrict__ rowptr, const void* __restri
   }
 }
 
-// Wide multivectors: lanes map to columns.  A group of LPR = min(B, 32) lanes
-// owns one row; every lane of the group reads the same 16-byte entry (one
-// broadcast transaction) and the group reads each X_j row as one coalesced
-// segment, so gathers cost 3 warp-wide loads per entry instead of 3*B scalar
-// loads per lane.  No shuffles: each lane accumulates its own columns.
-template <class T, int B>
-__global__ void __launch_bounds__(kThreads)
+// Wide multivectors: lanes map to columns.  A group of LPR lanes owns one row;
+// each lane owns V consecutive columns per chunk (V = 2 -> float2/double2 loads).
+// Every lane of the group reads the same 16-byte entry (one broadcast
+// transaction) and the group reads each X_j row as one coalesced segment.
+// Each block walks one contiguous slab of rows (its warps on neighbouring rows at
+// the same time), so the X_j rows shared by neighbouring atoms are reused from
+// L1.  No shuffles: each lane accumulates its own columns.
+template <class T, int V>
+struct VecT;
+template <>
+struct VecT<float, 1> {
+  using t = float;
+};
+template <>
+struct VecT<float, 2> {
+  using t = float2;
+};
+template <>
+struct VecT<double, 1> {
+  using t = double;
+};
+template <>
+struct VecT<double, 2> {
+  using t = double2;
+};
+
+template <class T, int V>
+__device__ __forceinline__ void vld(const T* p, T (&x)[V]) {
+  if constexpr (V == 1) {
+    x[0] = __ldg(p);
+  } else {
+    const typename VecT<T, 2>::t v = __ldg(reinterpret_cast<const typename VecT<T, 2>::t*>(p));
+    x[0] = v.x;
+    x[1] = v.y;
+  }
+}
+
+template <class T, int B, int V, int NT>
+__global__ void __launch_bounds__(NT)
 k_spmm_cols(int64_t n_atoms, const int64_t* __restrict__ rowptr, const void* __restrict__ ent,
             const T* __restrict__ diag, const T* __restrict__ X, int64_t ldx, T* Y, int64_t ldy, const T* Yin,
             int64_t ldyin, T* __restrict__ Acc, int64_t ldacc, int c0, Epi ep, const double* __restrict__ Q,
             int64_t ndof, const double* __restrict__ coef) {
-  constexpr int LPR = B < 32 ? B : 32;
-  constexpr int CPL = B / LPR;
+  constexpr int LPR = (B / V) < 32 ? (B / V) : 32;
+  constexpr int CPL = B / (LPR * V);
   constexpr int RPW = 32 / LPR;
-  constexpr int RPB = (kThreads / 32) * RPW;
+  constexpr int GPB = (NT / 32) * RPW;
   __shared__ double s_coef[8 * B];
   if (ep.r > 0) {
-    for (int t = threadIdx.x; t < ep.r * B; t += kThreads) s_coef[t] = coef[t];
+    for (int t = threadIdx.x; t < ep.r * B; t += NT) s_coef[t] = coef[t];
     __syncthreads();
   }
   const int lane = threadIdx.x & 31;
   const int cl = lane % LPR;
-  const int64_t first = (int64_t)blockIdx.x * RPB + (threadIdx.x >> 5) * RPW + lane / LPR;
-  for (int64_t i = first; i < n_atoms; i += (int64_t)gridDim.x * RPB) {
-    T acc[3][CPL];
+  const int grp = (threadIdx.x >> 5) * RPW + lane / LPR;
+  const int64_t per = (n_atoms + gridDim.x - 1) / gridDim.x;
+  const int64_t r_beg = (int64_t)blockIdx.x * per;
+  const int64_t r_end = r_beg + per < n_atoms ? r_beg + per : n_atoms;
+  for (int64_t i = r_beg + grp; i < r_end; i += GPB) {
+    T acc[3][CPL][V];
 #pragma unroll
-    for (int t = 0; t < CPL; ++t) acc[0][t] = acc[1][t] = acc[2][t] = T(0);
+    for (int t = 0; t < CPL; ++t)
+#pragma unroll
+      for (int v = 0; v < V; ++v) acc[0][t][v] = acc[1][t][v] = acc[2][t][v] = T(0);
     const int64_t e1 = rowptr[i + 1];
-    const T* Xc = X + c0 + cl;
-#pragma unroll 4
+    const T* Xc = X + c0 + cl * V;
+#pragma unroll 2
     for (int64_t e = rowptr[i]; e < e1; ++e) {
       T wx, wy, wz;
       int j;
@@ -154,11 +199,17 @@ k_spmm_cols(int64_t n_atoms, const int64_t* __restrict__ rowptr, const void* __r
       const T* xj = Xc + 3 * (int64_t)j * ldx;
 #pragma unroll
       for (int t = 0; t < CPL; ++t) {
-        const T x0 = __ldg(xj + t * LPR), x1 = __ldg(xj + ldx + t * LPR), x2 = __ldg(xj + 2 * ldx + t * LPR);
-        const T dot = wx * x0 + wy * x1 + wz * x2;
-        acc[0][t] -= wx * dot;
-        acc[1][t] -= wy * dot;
-        acc[2][t] -= wz * dot;
+        T x0[V], x1[V], x2[V];
+        vld<T, V>(xj + t * LPR * V, x0);
+        vld<T, V>(xj + ldx + t * LPR * V, x1);
+        vld<T, V>(xj + 2 * ldx + t * LPR * V, x2);
+#pragma unroll
+        for (int v = 0; v < V; ++v) {
+          const T dot = wx * x0[v] + wy * x1[v] + wz * x2[v];
+          acc[0][t][v] -= wx * dot;
+          acc[1][t][v] -= wy * dot;
+          acc[2][t][v] -= wz * dot;
+        }
       }
     }
     const T* d = diag + 8 * i;
@@ -166,21 +217,119 @@ k_spmm_cols(int64_t n_atoms, const int64_t* __restrict__ rowptr, const void* __r
     const int64_t r0 = 3 * i;
 #pragma unroll
     for (int t = 0; t < CPL; ++t) {
-      const int c = cl + t * LPR;
-      const T x0 = X[r0 * ldx + c0 + c], x1 = X[(r0 + 1) * ldx + c0 + c], x2 = X[(r0 + 2) * ldx + c0 + c];
-      T h[3];
-      h[0] = acc[0][t] + dxx * x0 + dxy * x1 + dxz * x2;
-      h[1] = acc[1][t] + dxy * x0 + dyy * x1 + dyz * x2;
-      h[2] = acc[2][t] + dxz * x0 + dyz * x1 + dzz * x2;
-      const T xs[3] = {x0, x1, x2};
 #pragma unroll
-      for (int a = 0; a < 3; ++a) {
-        const int64_t row = r0 + a;
-        double y = ep.alpha * (double)h[a] + ep.gamma * (double)xs[a];
-        if (ep.has_yin) y += ep.beta * (double)Yin[row * ldyin + c0 + c];
-        for (int q = 0; q < ep.r; ++q) y += Q[q * ndof + row] * s_coef[q * B + c];
-        Y[row * ldy + c0 + c] = (T)y;
-        if (ep.accumulate) Acc[row * ldacc + c0 + c] += (T)(ep.mu * y);
+      for (int v = 0; v < V; ++v) {
+        const int c = (t * LPR + cl) * V + v;
+        const T x0 = X[r0 * ldx + c0 + c], x1 = X[(r0 + 1) * ldx + c0 + c], x2 = X[(r0 + 2) * ldx + c0 + c];
+        T h[3];
+        h[0] = acc[0][t][v] + dxx * x0 + dxy * x1 + dxz * x2;
+        h[1] = acc[1][t][v] + dxy * x0 + dyy * x1 + dyz * x2;
+        h[2] = acc[2][t][v] + dxz * x0 + dyz * x1 + dzz * x2;
+        const T xs[3] = {x0, x1, x2};
+#pragma unroll
+        for (int a = 0; a < 3; ++a) {
+          const int64_t row = r0 + a;
+          double y = ep.alpha * (double)h[a] + ep.gamma * (double)xs[a];
+          if (ep.has_yin) y += ep.beta * (double)Yin[row * ldyin + c0 + c];
+          for (int q = 0; q < ep.r; ++q) y += Q[q * ndof + row] * s_coef[q * B + c];
+          Y[row * ldy + c0 + c] = (T)y;
+          if (ep.accumulate) Acc[row * ldacc + c0 + c] += (T)(ep.mu * y);
+        }
+      }
+    }
+  }
+}
+
+// Whole-warp rows (B / V >= 32 columns per lane-row): the warp loads 32 entries of
+// its row at once (one coalesced 512-byte load), broadcasts them by shuffle and
+// issues the X_j gathers of U entries back to back, so U * 3 gathers per warp are
+// in flight instead of 3.  Tail slots use w = 0 and j = the row itself.
+template <class T, int B, int V, int U>
+__global__ void __launch_bounds__(kThreads)
+k_spmm_warp(int64_t n_atoms, const int64_t* __restrict__ rowptr, const void* __restrict__ ent,
+            const T* __restrict__ diag, const T* __restrict__ X, int64_t ldx, T* Y, int64_t ldy, const T* Yin,
+            int64_t ldyin, T* __restrict__ Acc, int64_t ldacc, int c0, Epi ep, const double* __restrict__ Q,
+            int64_t ndof, const double* __restrict__ coef) {
+  constexpr int CPL = B / (32 * V);
+  static_assert(CPL >= 1, "whole-warp rows need B / V >= 32");
+  constexpr int WPB = kThreads / 32;
+  __shared__ double s_coef[8 * B];
+  if (ep.r > 0) {
+    for (int t = threadIdx.x; t < ep.r * B; t += kThreads) s_coef[t] = coef[t];
+    __syncthreads();
+  }
+  const int lane = threadIdx.x & 31;
+  const int warp = threadIdx.x >> 5;
+  const int64_t per = (n_atoms + gridDim.x - 1) / gridDim.x;
+  const int64_t r_beg = (int64_t)blockIdx.x * per;
+  const int64_t r_end = r_beg + per < n_atoms ? r_beg + per : n_atoms;
+  for (int64_t i = r_beg + warp; i < r_end; i += WPB) {
+    T acc[3][CPL][V];
+#pragma unroll
+    for (int t = 0; t < CPL; ++t)
+#pragma unroll
+      for (int v = 0; v < V; ++v) acc[0][t][v] = acc[1][t][v] = acc[2][t][v] = T(0);
+    const int64_t e0 = rowptr[i], e1 = rowptr[i + 1];
+    const T* Xc = X + c0 + lane * V;
+    for (int64_t base = e0; base < e1; base += 32) {
+      const int cnt = (int)((e1 - base) < 32 ? (e1 - base) : 32);
+      T mx = T(0), my = T(0), mz = T(0);
+      int mj = static_cast<int>(i);
+      if (lane < cnt) Ent<T>::load(ent, base + lane, mx, my, mz, mj);
+      for (int k = 0; k < cnt; k += U) {
+        T wx[U], wy[U], wz[U];
+        T xv[U][3][CPL][V];
+#pragma unroll
+        for (int u = 0; u < U; ++u) {
+          wx[u] = __shfl_sync(0xffffffffu, mx, (k + u) & 31);
+          wy[u] = __shfl_sync(0xffffffffu, my, (k + u) & 31);
+          wz[u] = __shfl_sync(0xffffffffu, mz, (k + u) & 31);
+          const int j = __shfl_sync(0xffffffffu, mj, (k + u) & 31);
+          // slots past the end of the row carry w = 0 (lanes >= cnt loaded nothing)
+          const T* xj = Xc + 3 * (int64_t)j * ldx;
+#pragma unroll
+          for (int t = 0; t < CPL; ++t) {
+            vld<T, V>(xj + t * 32 * V, xv[u][0][t]);
+            vld<T, V>(xj + ldx + t * 32 * V, xv[u][1][t]);
+            vld<T, V>(xj + 2 * ldx + t * 32 * V, xv[u][2][t]);
+          }
+        }
+#pragma unroll
+        for (int u = 0; u < U; ++u)
+#pragma unroll
+          for (int t = 0; t < CPL; ++t)
+#pragma unroll
+            for (int v = 0; v < V; ++v) {
+              const T dot = wx[u] * xv[u][0][t][v] + wy[u] * xv[u][1][t][v] + wz[u] * xv[u][2][t][v];
+              acc[0][t][v] -= wx[u] * dot;
+              acc[1][t][v] -= wy[u] * dot;
+              acc[2][t][v] -= wz[u] * dot;
+            }
+      }
+    }
+    const T* d = diag + 8 * i;
+    const T dxx = d[0], dyy = d[1], dzz = d[2], dxy = d[3], dxz = d[4], dyz = d[5];
+    const int64_t r0 = 3 * i;
+#pragma unroll
+    for (int t = 0; t < CPL; ++t) {
+#pragma unroll
+      for (int v = 0; v < V; ++v) {
+        const int c = (t * 32 + lane) * V + v;
+        const T x0 = X[r0 * ldx + c0 + c], x1 = X[(r0 + 1) * ldx + c0 + c], x2 = X[(r0 + 2) * ldx + c0 + c];
+        T h[3];
+        h[0] = acc[0][t][v] + dxx * x0 + dxy * x1 + dxz * x2;
+        h[1] = acc[1][t][v] + dxy * x0 + dyy * x1 + dyz * x2;
+        h[2] = acc[2][t][v] + dxz * x0 + dyz * x1 + dzz * x2;
+        const T xs[3] = {x0, x1, x2};
+#pragma unroll
+        for (int a = 0; a < 3; ++a) {
+          const int64_t row = r0 + a;
+          double y = ep.alpha * (double)h[a] + ep.gamma * (double)xs[a];
+          if (ep.has_yin) y += ep.beta * (double)Yin[row * ldyin + c0 + c];
+          for (int q = 0; q < ep.r; ++q) y += Q[q * ndof + row] * s_coef[q * B + c];
+          Y[row * ldy + c0 + c] = (T)y;
+          if (ep.accumulate) Acc[row * ldacc + c0 + c] += (T)(ep.mu * y);
+        }
       }
     }
   }
@@ -234,11 +383,43 @@ cudaError_t launch_tile(int64_t n_atoms, const int64_t* rowptr, const void* ent,
     k_qx_final<<<1, 512, 0, stream>>>(partial, kQxBlocks, ep.r, B, hot_shift, coef);
   }
   if constexpr (G == 0) {
-    constexpr int LPR = B < 32 ? B : 32;
-    const int rows_per_block = (kThreads / 32) * (32 / LPR);
-    const int blocks = grid_for(n_atoms, rows_per_block, 148 * 64);
-    k_spmm_cols<T, B><<<blocks, kThreads, 0, stream>>>(n_atoms, rowptr, ent, diag, X, ldx, Y, ldy, Yin, ldyin, Acc,
-                                                       ldacc, c0, ep, Q, ndof, coef);
+    // Vector (V = 2) gathers need X, Y (and Yin / Acc when used) rows aligned to
+    // 2 elements: every leading dimension and the column offset even, bases aligned.
+    const uintptr_t al = 2 * sizeof(T);
+    bool vec = (ldx % 2 == 0) && (ldy % 2 == 0) && (c0 % 2 == 0) && ((uintptr_t)X % al == 0) &&
+               ((uintptr_t)Y % al == 0);
+    if (ep.has_yin) vec = vec && (ldyin % 2 == 0) && ((uintptr_t)Yin % al == 0);
+    if (ep.accumulate) vec = vec && (ldacc % 2 == 0) && ((uintptr_t)Acc % al == 0);
+    const int nt = g_cols_threads.load();
+    const int bps = g_cols_blocks_per_sm.load();
+#define COLS_LAUNCH(NTV)                                                                                     \
+  {                                                                                                           \
+    const int blocks = grid_for(n_atoms, 4 * NTV / 32, 148 * bps);                                            \
+    if (vec)                                                                                                  \
+      k_spmm_cols<T, B, 2, NTV><<<blocks, NTV, 0, stream>>>(n_atoms, rowptr, ent, diag, X, ldx, Y, ldy, Yin,   \
+                                                            ldyin, Acc, ldacc, c0, ep, Q, ndof, coef);       \
+    else                                                                                                      \
+      k_spmm_cols<T, B, 1, NTV><<<blocks, NTV, 0, stream>>>(n_atoms, rowptr, ent, diag, X, ldx, Y, ldy, Yin,   \
+                                                            ldyin, Acc, ldacc, c0, ep, Q, ndof, coef);       \
+  }
+    const int wmode = g_warp_kernel.load();
+    if (wmode > 0 && B >= 32 && (vec || B >= 32)) {
+      const int blocks = grid_for(n_atoms, kThreads / 32, 148 * bps);
+      if constexpr (B >= 64) {
+        if (vec)
+          k_spmm_warp<T, B, 2, 4><<<blocks, kThreads, 0, stream>>>(n_atoms, rowptr, ent, diag, X, ldx, Y, ldy, Yin,
+                                                                    ldyin, Acc, ldacc, c0, ep, Q, ndof, coef);
+        else
+          k_spmm_warp<T, B, 1, 4><<<blocks, kThreads, 0, stream>>>(n_atoms, rowptr, ent, diag, X, ldx, Y, ldy, Yin,
+                                                                    ldyin, Acc, ldacc, c0, ep, Q, ndof, coef);
+      } else if constexpr (B >= 32) {
+        k_spmm_warp<T, B, 1, 4><<<blocks, kThreads, 0, stream>>>(n_atoms, rowptr, ent, diag, X, ldx, Y, ldy, Yin,
+                                                                  ldyin, Acc, ldacc, c0, ep, Q, ndof, coef);
+      }
+    } else if (nt == 1024) COLS_LAUNCH(1024)
+    else if (nt == 512) COLS_LAUNCH(512)
+    else COLS_LAUNCH(256)
+#undef COLS_LAUNCH
   } else {
     const int rows_per_block = kThreads / G;
     const int blocks = grid_for(n_atoms, rows_per_block, 148 * 16);
@@ -265,8 +446,15 @@ cudaError_t run(int64_t n_atoms, const int64_t* rowptr, const void* ent, const v
   e = launch_tile<T, BB, GG>(n_atoms, rowptr, ent, D, X, ldx, Y, ldy, Yin, ldyin, Acc, ldacc, c0, ep, Q,     \
                              hot_shift, partial, coef, s);                                                     \
   c0 += BB;
-    if (rem >= 64 && sizeof(T) == 4) { TILE(64, 0) }
-    else if (rem >= 32) { TILE(32, 0) }
+    bool done64 = false;
+    if constexpr (sizeof(T) == 4) {
+      if (rem >= 64) {
+        TILE(64, 0)
+        done64 = true;
+      }
+    }
+    if (done64) {
+    } else if (rem >= 32) { TILE(32, 0) }
     else if (rem >= 16) { TILE(16, 0) }
     else if (rem >= 8) { TILE(8, 0) }
     else if (rem >= 4) { TILE(4, 8) }
@@ -281,6 +469,20 @@ cudaError_t run(int64_t n_atoms, const int64_t* rowptr, const void* ent, const v
 }  // namespace inch
 
 using namespace inch;
+
+extern "C" inch_status inch_spmm_tune(int32_t threads_per_block, int32_t blocks_per_sm) {
+  // threads_per_block 0 selects the whole-warp-row kernel (batched gathers) where it
+  // applies; 256/512/1024 select the lane-group kernel with that block size.
+  INCH_REQUIRE(threads_per_block == 0 || threads_per_block == 256 || threads_per_block == 512 ||
+                   threads_per_block == 1024,
+               INCH_INVALID_ARG, "inch_spmm_tune: threads_per_block must be 0, 256, 512 or 1024");
+  g_warp_kernel.store(threads_per_block == 0 ? 1 : 0);
+  if (threads_per_block == 0) threads_per_block = 256;
+  INCH_REQUIRE(blocks_per_sm >= 1 && blocks_per_sm <= 8, INCH_INVALID_ARG, "inch_spmm_tune: blocks_per_sm in 1..8");
+  g_cols_threads.store(threads_per_block);
+  g_cols_blocks_per_sm.store(blocks_per_sm);
+  return INCH_OK;
+}
 
 extern "C" size_t inch_spmm_workspace_size(int64_t n_atoms, int32_t b, int32_t r) {
   (void)n_atoms;

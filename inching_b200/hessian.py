@@ -50,7 +50,7 @@ class HessianStore:
     order the caller wants (normally reversed Cuthill-McKee)."""
 
     def __init__(self, X_nm, rc_gamma_A: float = 8.0, plus_i: float = 1.0, precisions=("f64", "f32"),
-                 device=None, graph_=None):
+                 device=None, graph_=None, tiles=False):
         self.X = graph.to_device_coords(X_nm, device)
         self.device = self.X.device
         self.n_atoms = int(self.X.shape[0])
@@ -69,6 +69,13 @@ class HessianStore:
         self.dtype = np.dtype(np.float64)
         self.nnz_blocks = int(self.cols.shape[0])
         self._diag_vec = None
+        # Row-tile layout of the same matrix for products with >= 8 columns.
+        self.tiles = None
+        self.use_tiles = bool(tiles)
+        if tiles:
+            uptr, pptr, urec, pw64, pw32, nu, npairs = _native.tile_store(self.X, self.rowptr, self.cols,
+                                                                          self.rc_nm, want64, want32)
+            self.tiles = dict(uptr=uptr, pptr=pptr, urec=urec, pw64=pw64, pw32=pw32, n_union=nu, n_pairs=npairs)
 
     # -- reference-compatible views ------------------------------------------------
     @property
@@ -91,10 +98,18 @@ class HessianStore:
             raise AssertionError("ABORTED. the FP32 store was not assembled")
         return self.ent32, self.diag32
 
-    def store_bytes(self, prec: int) -> int:
-        """Bytes one SpMM pass streams from the store (entries + diagonal + rowptr)."""
+    def store_bytes(self, prec: int, b: int = 1) -> int:
+        """Bytes one SpMM pass streams from the store for a b-column product: the
+        row-tile layout for b >= 8 when built (records + w + offsets + diagonal),
+        else the pair layout (entries + diagonal + rowptr)."""
         ent, diag = self.store(prec)
-        return ent.numel() * ent.element_size() + diag.numel() * diag.element_size() + 8 * (self.n_atoms + 1)
+        dbytes = diag.numel() * diag.element_size()
+        if b >= 8 and self.tiles is not None and self.use_tiles:
+            t = self.tiles
+            pw = t["pw64"] if prec == 64 else t["pw32"]
+            return (t["n_union"] * 4 + t["n_pairs"] * pw.shape[1] * pw.element_size()
+                    + 16 * (t["uptr"].numel()) + dbytes)
+        return ent.numel() * ent.element_size() + dbytes + 8 * (self.n_atoms + 1)
 
     # -- products ---------------------------------------------------------------
     def matmul(self, X, out=None, prec=None, **epilogue):
@@ -104,6 +119,19 @@ class HessianStore:
         want = torch.float64 if prec == 64 else torch.float32
         if X.dtype != want:
             raise AssertionError(f"ABORTED. prec {prec} needs {want} vectors, got {X.dtype}")
+        if (X.dim() == 2 and X.shape[1] >= 8 and X.shape[1] % 8 != 0 and epilogue.get("Yin") is None
+                and epilogue.get("acc") is None):
+            # pad the block to a multiple of 8 columns so every column tile runs the
+            # vector-gather kernel on aligned rows; the zero columns cost < 8 columns
+            b = X.shape[1]
+            bp = (b + 7) // 8 * 8
+            Xp = torch.zeros((X.shape[0], bp), dtype=X.dtype, device=X.device)
+            Xp[:, :b] = X
+            Yp = self.matmul(Xp, prec=prec, **epilogue)
+            if out is None:
+                return Yp[:, :b].contiguous()
+            out.copy_(Yp[:, :b])
+            return out
         if out is None:
             out = torch.empty_like(X)
         ent, diag = self.store(prec)
@@ -111,7 +139,7 @@ class HessianStore:
         if probe is not None:
             b = 1 if X.dim() == 1 else X.shape[1]
             vec = X.element_size() * X.shape[0] * b
-            nbytes = self.store_bytes(prec) + vec * (2 + (epilogue.get("Yin") is not None)
+            nbytes = self.store_bytes(prec, b) + vec * (2 + (epilogue.get("Yin") is not None)
                                                      + 2 * (epilogue.get("acc") is not None))
             ev0 = torch.cuda.Event(enable_timing=True)
             ev1 = torch.cuda.Event(enable_timing=True)
@@ -123,6 +151,19 @@ class HessianStore:
         return self._matmul(prec, ent, diag, X, out, epilogue)
 
     def _matmul(self, prec, ent, diag, X, out, epilogue):
+        if X.dim() == 2 and X.shape[1] >= 8 and self.tiles is not None and self.use_tiles:
+            t = self.tiles
+            pw = t["pw64"] if prec == 64 else t["pw32"]
+            if pw is not None:
+                for c0 in range(0, X.shape[1], 64):
+                    sl = slice(c0, min(c0 + 64, X.shape[1]))
+                    kw = dict(epilogue)
+                    for key in ("Yin", "acc"):
+                        if kw.get(key) is not None:
+                            kw[key] = kw[key][:, sl]
+                    _native.spmm_tiles(prec, self.n_atoms, t["uptr"], t["pptr"], t["urec"], pw, diag, X[:, sl],
+                                       out[:, sl], **kw)
+                return out
         if X.dim() == 1 or X.shape[1] <= 64:
             return _native.spmm(prec, self.n_atoms, self.rowptr, ent, diag, X, out, **epilogue)
         # the kernel takes up to 64 columns per call: walk column panels

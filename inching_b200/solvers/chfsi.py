@@ -72,7 +72,10 @@ class _Filter:
         sigma = e / (a0 - c)
         sigma1 = sigma
         tau = 2.0 / sigma1
-        X = X64.to(dt).clone()         # the recurrence overwrites X
+        b = X64.shape[1]
+        bp = (b + 7) // 8 * 8          # aligned width for the vector-gather SpMM
+        X = torch.zeros((X64.shape[0], bp), dtype=dt, device=X64.device)
+        X[:, :b] = X64                 # fresh buffer: the recurrence overwrites X
         Y = torch.empty_like(X)
         self.A.matmul(X, out=Y, prec=self.prec, alpha=sigma1 / e, gamma=-sigma1 * c / e)
         self.n_spmm += 1
@@ -84,7 +87,7 @@ class _Filter:
             X, Y = Y, X
             sigma = s2
             self.n_spmm += 1
-        return Y.to(torch.float64)
+        return Y[:, :b].to(torch.float64)
 
 
 def _rr(A, Y, prec):

@@ -157,6 +157,13 @@ typedef struct {
 } inch_spmm_epilogue;
 
 size_t inch_spmm_workspace_size(int64_t n_atoms, int32_t b, int32_t r);
+/* Launch shape of the wide-block (b >= 8) SpMM kernel for this process: threads
+ * per block (256, 512 or 1024) and resident blocks per SM (1..8); each block walks
+ * one contiguous slab of rows.  threads_per_block = 0 selects instead, for tiles of
+ * >= 32 columns per lane-row, the whole-warp-row kernel that loads 32 entries at
+ * once and batches 4 entries' gathers.  Hook of the autotuner (inching_b200.autotune);
+ * default 256 x 5.  No reference counterpart. */
+inch_status inch_spmm_tune(int32_t threads_per_block, int32_t blocks_per_sm);
 inch_status inch_spmm(int32_t prec, int64_t n_atoms, const int64_t* rowptr_dev,
                       const void* ent_dev, const void* diag_dev,
                       const void* X_dev, int64_t ldx, int32_t b,
@@ -165,6 +172,32 @@ inch_status inch_spmm(int32_t prec, int64_t n_atoms, const int64_t* rowptr_dev,
                       const double* q_dev /* (r, 3N) row-major, FP64 */,
                       const inch_spmm_epilogue* ep,
                       void* ws_dev, size_t ws_bytes, cudaStream_t stream);
+
+/* ---------------------------------------------------------------------------
+ * Row-tile store for wide multivectors (no reference counterpart; an alternative
+ * layout of the same matrix).  Atoms are grouped in tiles of 8 consecutive rows;
+ * per tile, the merged sorted union of the rows' neighbour columns is stored as
+ * urec = (j << 8) | row-mask, followed in pw by w = x/|x| for every set mask bit
+ * (FP64 {wx,wy,wz,0} 32 B, FP32 {wx,wy,wz,0} 16 B); self pairs are omitted.
+ * tile_uptr / tile_pptr: (n_tiles + 1) offsets.  n_atoms < 2^24.
+ * count (synchronises, returns the totals) then fill; inch_spmm_tiles is
+ * inch_spmm on this layout (same epilogue, diagonal from inch_hessian_assemble).
+ * ------------------------------------------------------------------------- */
+size_t inch_tile_store_workspace_size(int64_t n_atoms);
+inch_status inch_tile_store_count(const int64_t* rowptr_dev, const int32_t* cols_dev, int64_t n_atoms,
+                                  int64_t* tile_uptr_dev, int64_t* tile_pptr_dev, int64_t* n_union_host,
+                                  int64_t* n_pairs_host, void* ws_dev, size_t ws_bytes, cudaStream_t stream);
+inch_status inch_tile_store_fill(const double* X_dev, int64_t n_atoms, double rc, const int64_t* rowptr_dev,
+                                 const int32_t* cols_dev, const int64_t* tile_uptr_dev,
+                                 const int64_t* tile_pptr_dev, uint32_t* urec_dev, double* pw64_dev,
+                                 float* pw32_dev, cudaStream_t stream);
+size_t inch_spmm_tiles_workspace_size(void);
+inch_status inch_spmm_tiles(int32_t prec, int64_t n_atoms, const int64_t* tile_uptr_dev,
+                            const int64_t* tile_pptr_dev, const uint32_t* urec_dev, const void* pw_dev,
+                            const void* diag_dev, const void* X_dev, int64_t ldx, int32_t b,
+                            void* Y_dev, int64_t ldy, const void* Yin_dev, int64_t ldyin,
+                            void* Acc_dev, int64_t ldacc, const double* q_dev,
+                            const inch_spmm_epilogue* ep, void* ws_dev, size_t ws_bytes, cudaStream_t stream);
 
 /* Allocation-free form of inch_spmm (no counterpart in the reference).  For
  * callers that cannot provide device scratch -- hosts running on another

@@ -107,3 +107,46 @@ def test_full_size_store_properties():
     v = torch.randn(H.shape[0], 2, dtype=torch.float64, device="cuda").contiguous()
     Hv = H.matmul(v)
     assert abs(float(v[:, 0] @ Hv[:, 1] - v[:, 1] @ Hv[:, 0])) < 1e-8 * float(v[:, 0] @ Hv[:, 0])
+
+
+@pytest.mark.parametrize("prec", [64, 32])
+def test_spmm_unaligned_rows_scalar_gather(case, prec):
+    """Odd leading dimension (rows not 2-element aligned): the column kernel falls
+    back to scalar gathers and must give the same product."""
+    from inching_b200 import _native
+    Xr, H, A, Ad, Hfull, Q = case
+    b, ld = 24, 25
+    rng = np.random.default_rng(11)
+    Xv = rng.standard_normal((H.shape[0], ld))
+    ref = np.stack([oh.krylov_av(A, Ad, Xv[:, c]) for c in range(b)], axis=1)
+    dt = torch.float64 if prec == 64 else torch.float32
+    Xt = torch.from_numpy(Xv).to("cuda", dt)
+    Yt = torch.zeros_like(Xt)
+    ent, diag = H.store(prec)
+    _native.spmm(prec, H.n_atoms, H.rowptr, ent, diag, Xt[:, :b], Yt[:, :b])
+    tol = (TOL64 if prec == 64 else TOL32) * abs(Hfull).max() * np.abs(Xv).max() * 10
+    assert np.abs(Yt[:, :b].double().cpu().numpy() - ref).max() <= tol
+    assert float(Yt[:, b:].abs().max()) == 0.0
+
+
+@pytest.mark.parametrize("prec", [64, 32])
+@pytest.mark.parametrize("b", [8, 40, 64])
+def test_row_tile_layout_matches_oracle(case, prec, b):
+    """The optional row-tile layout (8-row tiles, merged neighbour unions) gives the
+    same products as the oracle, with the fused epilogue."""
+    from inching_b200.hessian import HessianStore
+    Xr, H, A, Ad, Hfull, Q = case
+    Ht = HessianStore(Xr, 8.0, plus_i=1.0, tiles=True)
+    assert Ht.tiles["n_pairs"] == Ht.nnz_blocks - Ht.n_atoms
+    rng = np.random.default_rng(b)
+    Xv = rng.standard_normal((H.shape[0], b))
+    Yin = rng.standard_normal((H.shape[0], b))
+    HX = np.stack([oh.krylov_av(A, Ad, Xv[:, c]) for c in range(b)], axis=1)
+    ref = 0.5 * HX - 0.25 * Xv - Yin + 10.0 * Q.T @ (Q @ Xv)
+    dt = torch.float64 if prec == 64 else torch.float32
+    Xt = torch.from_numpy(Xv).to("cuda", dt).contiguous()
+    Yt = torch.from_numpy(Yin).to("cuda", dt).contiguous()
+    Ht.matmul(Xt, out=Yt, prec=prec, alpha=0.5, gamma=-0.25, beta=-1.0, Yin=Yt,
+              Q=torch.from_numpy(Q).cuda(), hot_shift=10.0)
+    tol = (TOL64 if prec == 64 else TOL32) * abs(Hfull).max() * np.abs(Xv).max() * 50
+    assert np.abs(Yt.double().cpu().numpy() - ref).max() <= tol
