@@ -43,8 +43,12 @@ def _solve(H, k, solver, precision, tol, Q, shift, seed, **kw):
 
 
 def normal_modes_device(X_nm: torch.Tensor, k: int, *, rc_gamma_A=8.0, plus_i=1.0, solver="chfsi",
-                        precision="mixed", tol=1e-6, deflate_rigid=True, hotelling_shift=10.0, seed=0, **kw):
+                        precision="mixed", tol=1e-6, deflate_rigid=True, hotelling_shift=10.0, seed=0,
+                        warm_start=None, **kw):
     """Lowest k non-rigid modes of the structure X_nm (CUDA (N,3) float64, nm).
+
+    warm_start="coarse" (block solver only): initial block from the lowest modes
+    of a bead model of the structure (inching_b200.warmstart).
 
     tol: for "chfsi", the relative residual ||Hv - lambda v|| <= tol*||H||; for the
     reference solvers, their own absolute tolerance.  Returns (eigval (k,) with
@@ -55,14 +59,38 @@ def normal_modes_device(X_nm: torch.Tensor, k: int, *, rc_gamma_A=8.0, plus_i=1.
     precisions = ("f64", "f32") if precision == "mixed" else ("f64",)
     H = HessianStore(Xr, rc_gamma_A, plus_i=plus_i, precisions=precisions)
     Q = rigid_body_basis(Xr) if deflate_rigid else None
+    winfo = None
+    if warm_start == "coarse":
+        if solver != "chfsi":
+            raise AssertionError("ABORTED. warm_start='coarse' is available for solver='chfsi'")
+        from .warmstart import coarse_warm_start
+        from .solvers.chfsi import default_guard
+        kw["X0"], winfo = coarse_warm_start(Xr, k + default_guard(k), seed=seed, return_info=True)
+    elif warm_start is not None:
+        raise AssertionError(f"ABORTED. unknown warm_start {warm_start!r}")
     t1 = time.perf_counter()
     evals, evecs, info = _solve(H, k, solver, precision, tol, Q, hotelling_shift, seed, **kw)
     n_atoms = Xr.shape[0]
     modes = evecs.t().reshape(evecs.shape[1], n_atoms, 3)[:, undo, :]
     info = dict(info)
     info.update(dict(n_atoms=int(n_atoms), nnz_blocks=H.nnz_blocks, rcm_levels=levels,
-                     mean_degree=float(degree.double().mean()), setup_s=t1 - t0))
+                     mean_degree=float(degree.double().mean()), setup_s=t1 - t0, warm_start=winfo))
     return evals - plus_i, modes, info
+
+
+_pinned = {}
+
+
+def _pinned_buffer(shape, dtype):
+    """Reusable page-locked host buffer (allocating 100s of MB of pinned memory
+    per call costs more than the copy itself)."""
+    key = (tuple(shape), dtype)
+    buf = _pinned.get(key)
+    if buf is None:
+        _pinned.clear()
+        buf = torch.empty(shape, dtype=dtype, pin_memory=True)
+        _pinned[key] = buf
+    return buf
 
 
 def normal_modes(X, k: int, *, units="nm", **kw):
@@ -75,6 +103,6 @@ def normal_modes(X, k: int, *, units="nm", **kw):
     Xd = torch.from_numpy(np.ascontiguousarray(Xh)).pin_memory().to("cuda", non_blocking=True)
     evals, modes, info = normal_modes_device(Xd, k, **kw)
     ev = evals.cpu().numpy()
-    out = torch.empty(modes.shape, dtype=modes.dtype, pin_memory=True)
+    out = _pinned_buffer(modes.shape, modes.dtype)
     out.copy_(modes)
-    return ev, out.numpy(), info
+    return ev, out.numpy().copy(), info

@@ -36,16 +36,24 @@ from ..krylov import HessianOperator
 from ..spectrum import estimate_spectrum_bound
 
 
+def default_guard(k):
+    """Guard vectors carried beyond the k wanted ones (a quarter of k, at least 16:
+    the gap to the block's last Ritz value sets the filter's convergence rate)."""
+    return max(16, int(math.ceil(0.25 * k)))
+
+
 def _cholqr(Y):
-    """Orthonormalise columns of Y (FP64) by Cholesky-QR applied twice."""
+    """Orthonormalise columns of Y (FP64) by Cholesky-QR applied twice.  The
+    triangular factor is inverted on the small (p, p) side so that the tall
+    update is one GEMM; Householder QR if the Gram matrix is not positive."""
     for _ in range(2):
         G = Y.t() @ Y
-        try:
-            R = torch.linalg.cholesky(G, upper=True)
-        except RuntimeError:
+        R, info = torch.linalg.cholesky_ex(G, upper=True)
+        if int(info) != 0:
             Qf, _ = torch.linalg.qr(Y)
             return Qf
-        Y = torch.linalg.solve_triangular(R, Y, upper=True, left=False)
+        Rinv = torch.linalg.solve_triangular(R, torch.eye(R.shape[0], dtype=R.dtype, device=R.device), upper=True)
+        Y = Y @ Rinv
     return Y
 
 
@@ -103,8 +111,41 @@ def _rr(A, Y, prec):
     return th, Y @ Wd, HY @ Wd
 
 
+class _Phases:
+    """CUDA-event timing of the solver phases (enabled with profile=True)."""
+
+    def __init__(self, on):
+        self.on = on
+        self.ev = {}
+
+    def __call__(self, name):
+        return _Span(self, name)
+
+    def summary(self):
+        if not self.on:
+            return None
+        torch.cuda.synchronize()
+        return {k: round(sum(a.elapsed_time(b) for a, b in v), 2) for k, v in self.ev.items()}
+
+
+class _Span:
+    def __init__(self, ph, name):
+        self.ph, self.name = ph, name
+
+    def __enter__(self):
+        if self.ph.on:
+            self.a = torch.cuda.Event(enable_timing=True)
+            self.a.record()
+
+    def __exit__(self, *x):
+        if self.ph.on:
+            b = torch.cuda.Event(enable_timing=True)
+            b.record()
+            self.ph.ev.setdefault(self.name, []).append((self.a, b))
+
+
 def chfsi(A, k, tol=1e-6, Q=None, precision="mixed", degree=24, guard=None, maxiter=300, X0=None, seed=0,
-          spectrum_upper=None, final_f64=True, verbose=False, return_info=False):
+          spectrum_upper=None, final_f64=True, verbose=False, return_info=False, profile=False):
     """Lowest k eigenpairs of A (+PlusI) orthogonal to the rows of Q.
 
     tol is relative: a pair is locked when ||H y - theta y|| <= tol * ||H||, with
@@ -117,11 +158,13 @@ def chfsi(A, k, tol=1e-6, Q=None, precision="mixed", degree=24, guard=None, maxi
     assert precision in ("f64", "mixed"), "ABORTED. precision must be 'f64' or 'mixed'"
     prec = 32 if precision == "mixed" else 64
     if guard is None:
-        guard = max(16, int(math.ceil(0.15 * k)))
+        guard = default_guard(k)
     p = min(k + guard, n - (0 if Q is None else Q.shape[0]))
     Qd = None if Q is None else HessianOperator(A, Q=Q).Q
+    ph = _Phases(profile)
     if spectrum_upper is None:
-        lo, hi = estimate_spectrum_bound(A, steps=40, seed=seed + 1, precision=precision)
+        with ph("bound"):
+            lo, hi = estimate_spectrum_bound(A, steps=40, seed=seed + 1, precision=precision)
         spectrum_upper = hi * 1.02 + 1e-3 * abs(hi)
     b_up = float(spectrum_upper)
     normH = b_up
@@ -132,8 +175,10 @@ def chfsi(A, k, tol=1e-6, Q=None, precision="mixed", degree=24, guard=None, maxi
         X0 = X0.to(device=dev, dtype=torch.float64)
         c0 = min(X0.shape[1], p)
         Y[:, :c0] = X0[:, :c0]
-    Y = _cholqr(_project_out(Y, Qd))
-    th, Y, HY = _rr(A, Y, prec)
+    with ph("orth"):
+        Y = _cholqr(_project_out(Y, Qd))
+    with ph("rr"):
+        th, Y, HY = _rr(A, Y, prec)
     filt = _Filter(A, prec)
     locked = torch.empty((0, n), dtype=torch.float64, device=dev)   # rows
     locked_theta = []
@@ -141,8 +186,9 @@ def chfsi(A, k, tol=1e-6, Q=None, precision="mixed", degree=24, guard=None, maxi
     n_rr = 1
     res = np.full(p, np.inf)
     for it in range(maxiter):
-        R = HY - Y * torch.from_numpy(th).to(dev)[None, :]
-        res = torch.linalg.vector_norm(R, dim=0).cpu().numpy()
+        with ph("residual"):
+            R = HY - Y * torch.from_numpy(th).to(dev)[None, :]
+            res = torch.linalg.vector_norm(R, dim=0).cpu().numpy()
         want = k - locked.shape[0]
         nl = 0
         while nl < min(want, Y.shape[1]) and res[nl] <= tol * normH:
@@ -160,11 +206,14 @@ def chfsi(A, k, tol=1e-6, Q=None, precision="mixed", degree=24, guard=None, maxi
         a0 = float(min(th[0], locked_theta[0] if locked_theta else th[0]))
         if not (a0 < a < b_up):
             a0 = a - 1e-3 * abs(a)
-        Z = filt(Y, degree, a, b_up, a0 - 1e-12)
-        Z = _project_out(Z, Qd)
-        Z = _project_out(Z, locked)
-        Z = _cholqr(Z)
-        th, Y, HY = _rr(A, Z, prec)
+        with ph("filter"):
+            Z = filt(Y, degree, a, b_up, a0 - 1e-12)
+        with ph("orth"):
+            Z = _project_out(Z, Qd)
+            Z = _project_out(Z, locked)
+            Z = _cholqr(Z)
+        with ph("rr"):
+            th, Y, HY = _rr(A, Z, prec)
         n_rr += 1
     converged = locked.shape[0] >= k
     if not converged:
@@ -174,7 +223,8 @@ def chfsi(A, k, tol=1e-6, Q=None, precision="mixed", degree=24, guard=None, maxi
         locked_theta.extend(th[:extra].tolist())
     L = locked[:k].t().contiguous()
     if final_f64:
-        th_f, L, HL = _rr(A, L, 64)
+        with ph("final_f64"):
+            th_f, L, HL = _rr(A, L, 64)
         R = HL - L * torch.from_numpy(th_f).to(dev)[None, :]
         final_res = torch.linalg.vector_norm(R, dim=0).cpu().numpy() / normH
         evals = th_f
@@ -189,6 +239,6 @@ def chfsi(A, k, tol=1e-6, Q=None, precision="mixed", degree=24, guard=None, maxi
         info = dict(iterations=it + 1, converged=converged, n_spmm_filter=filt.n_spmm, n_rr=n_rr,
                     normH=normH, degree=degree, block=p,
                     max_rel_residual=None if final_res is None else float(final_res.max()),
-                    seconds=time.perf_counter() - t_start)
+                    seconds=time.perf_counter() - t_start, phases_ms=ph.summary())
         return evals_t, L, info
     return evals_t, L
