@@ -67,6 +67,8 @@ _SIGS = {
                                              c_void_p, c_void_p, c_void_p, c_void_p, c_void_p]),
     "inch_spmm_workspace_size": (c_size_t, [c_int64, c_int32, c_int32]),
     "inch_spmm_tune": (ctypes.c_int, [c_int32, c_int32]),
+    "inch_spmm_seg": (ctypes.c_int, [c_int32, c_int64, c_void_p, c_void_p, c_void_p, c_void_p, c_int64, c_int32,
+                                     c_void_p, c_int64, c_void_p, c_int64, c_void_p, c_void_p, c_void_p]),
     "inch_spmm": (ctypes.c_int, [c_int32, c_int64, c_void_p, c_void_p, c_void_p, c_void_p, c_int64, c_int32,
                                  c_void_p, c_int64, c_void_p, c_int64, c_void_p, c_int64, c_void_p,
                                  POINTER(SpmmEpilogue), c_void_p, c_size_t, c_void_p]),
@@ -220,6 +222,26 @@ def hessian_assemble(X, rowptr, cols, rc_nm, plus_i, want64=True, want32=True):
 
 
 _ws_cache = {}
+
+
+def spmm_seg(prec, n_atoms, rowptr, ent, diag, X, Y, atom_seg, seg_coef, Yin=None):
+    """Y = alpha_s (H X) + gamma_s X + beta_s Yin with (alpha, gamma, beta) per segment s
+    of atom i (atom_seg int32 (N,), seg_coef float64 (S, 3)).  X, Y: (3N, b), b <= 64."""
+    L = lib()
+    b = 1 if X.dim() == 1 else X.shape[1]
+    ldx = 1 if X.dim() == 1 else X.stride(0)
+    ldy = 1 if Y.dim() == 1 else Y.stride(0)
+    ldyin = 0 if Yin is None else (1 if Yin.dim() == 1 else Yin.stride(0))
+    check(L.inch_spmm_seg(prec, n_atoms, _ptr(rowptr), _ptr(ent), _ptr(diag), _ptr(X), ldx, b, _ptr(Y), ldy,
+                          _ptr(Yin), ldyin, _ptr(atom_seg), _ptr(seg_coef), _stream()))
+    tiles = 0
+    rem = b
+    for t in ((64, 32, 16, 8, 4, 2, 1) if prec == 32 else (32, 16, 8, 4, 2, 1)):
+        while rem >= t:
+            rem -= t
+            tiles += 1
+    _count(tiles)
+    return Y
 
 
 def spmm_tune(threads_per_block=256, blocks_per_sm=5):

@@ -16,7 +16,7 @@ import time
 import numpy as np
 import torch
 
-from .deflation import rigid_body_basis
+from .deflation import rigid_body_basis_padded
 from .hessian import HessianStore
 from .solvers.batched import chfsi_batched
 
@@ -48,15 +48,40 @@ def lattice_layout(structs_nm, rc_nm):
     return np.concatenate(parts, axis=0)
 
 
+def _bucket_warm_start(Xd, sid, n_struct, k, guard, seed, bead_edge_A=6.0, rc_bead_A=12.0):
+    """Per-structure bead models of a laid-out bucket, solved together (their bead
+    Hessian is block-diagonal too), prolonged to the atoms: (3N, m) FP64."""
+    edge = bead_edge_A / 10.0
+    lo = Xd.min(dim=0).values
+    c = torch.floor((Xd - lo) / edge).long()
+    dims = c.max(dim=0).values + 1
+    key = ((sid * dims[0] + c[:, 0]) * dims[1] + c[:, 1]) * dims[2] + c[:, 2]
+    uniq, bead = torch.unique(key, return_inverse=True)       # sorted: beads grouped by structure
+    nb = uniq.shape[0]
+    one = torch.ones_like(bead, dtype=torch.float64)
+    cnt = torch.zeros(nb, dtype=torch.float64, device=Xd.device).index_add_(0, bead, one)
+    pos = torch.zeros((nb, 3), dtype=torch.float64, device=Xd.device).index_add_(0, bead, Xd) / cnt[:, None]
+    bead_sid = torch.zeros(nb, dtype=torch.long, device=Xd.device).index_copy_(0, bead, sid)
+    nbs = torch.bincount(bead_sid, minlength=n_struct).cpu().numpy()
+    boff = np.concatenate([[0], np.cumsum(nbs)])
+    Hb = HessianStore(pos, rc_bead_A, plus_i=1.0)
+    m = int(min(k + guard, 3 * nbs.min() - 7))
+    Qb = rigid_body_basis_padded(pos, boff, int(3 * nbs.max()))
+    _, Vb, _ = chfsi_batched(Hb, 3 * boff, m - 2, tol=1e-3, Qp=Qb, precision="mixed", guard=2, seed=seed + 7)
+    return Vb.reshape(nb, 3, -1).index_select(0, bead).reshape(3 * Xd.shape[0], -1)
+
+
 def batched_normal_modes(structs, k=32, *, units="nm", rc_gamma_A=8.0, plus_i=1.0, tol=1e-6, precision="mixed",
-                         degree=24, bucket_ratio=1.6, seed=0, verbose=False):
+                         degree=24, bucket_ratio=1.6, seed=0, verbose=False, profile=False, warm_start=None):
     t0 = time.perf_counter()
     structs = [np.asarray(X, dtype=np.float64) / (10.0 if units == "A" else 1.0) for X in structs]
     sizes = np.array([X.shape[0] for X in structs])
     results = [None] * len(structs)
     infos = []
     rc = rc_gamma_A / 10.0
+    import time as _t
     for bucket in buckets_by_size(sizes, bucket_ratio):
+        tb0 = _t.perf_counter()
         Xcat = lattice_layout([structs[i] for i in bucket], rc)
         Xd = torch.from_numpy(Xcat).cuda()
         precisions = ("f64", "f32") if precision == "mixed" else ("f64",)
@@ -69,19 +94,27 @@ def batched_normal_modes(structs, k=32, *, units="nm", rc_gamma_A=8.0, plus_i=1.
         if not bool((sid[H.cols.long()] == rows).all()):
             raise AssertionError("ABORTED. structures overlap in the batched layout")
         n_max = int(3 * sizes[bucket].max())
-        Qp = torch.zeros((len(bucket), 6, n_max), dtype=torch.float64, device=Xd.device)
-        for t in range(len(bucket)):
-            a0, a1 = int(atom_off[t]), int(atom_off[t + 1])
-            Qp[t, :, :3 * (a1 - a0)] = rigid_body_basis(Xd[a0:a1])
+        Qp = rigid_body_basis_padded(Xd, atom_off, n_max)
+        Y0 = None
+        if warm_start == "coarse":
+            guard = max(16, int(np.ceil(0.5 * k)))
+            Y0 = _bucket_warm_start(Xd, sid, len(bucket), k, guard, seed)
+        if profile:
+            torch.cuda.synchronize()
+        tb1 = _t.perf_counter()
         ev, V, info = chfsi_batched(H, 3 * atom_off, k, tol=tol, Qp=Qp, precision=precision, degree=degree,
-                                    seed=seed, verbose=verbose)
+                                    seed=seed, verbose=verbose, profile=profile, Y0=Y0)
+        if profile:
+            torch.cuda.synchronize()
+        tb2 = _t.perf_counter()
         ev = ev.cpu().numpy()
         for t, i in enumerate(bucket):
             a0, a1 = int(atom_off[t]), int(atom_off[t + 1])
             modes = V[3 * a0:3 * a1].t().reshape(k, a1 - a0, 3)
             results[i] = (ev[t] - plus_i, modes)
         info = dict(info)
-        info.update(n_atoms=int(atom_off[-1]), sizes=(int(sizes[bucket].min()), int(sizes[bucket].max())))
+        info.update(n_atoms=int(atom_off[-1]), sizes=(int(sizes[bucket].min()), int(sizes[bucket].max())),
+                    setup_s=round(tb1 - tb0, 3), solve_s=round(tb2 - tb1, 3))
         infos.append(info)
     torch.cuda.synchronize()
     return results, dict(buckets=infos, seconds=time.perf_counter() - t0, structures=len(structs))

@@ -25,6 +25,9 @@ namespace {
 struct Epi {
   double alpha, gamma, beta, mu;
   int r, accumulate, has_yin;
+  // optional per-segment (alpha, gamma, beta): atom i uses seg_coef[3 * atom_seg[i] ...]
+  const double* seg_coef = nullptr;
+  const int* atom_seg = nullptr;
 };
 
 template <class T>
@@ -115,8 +118,15 @@ k_spmm(int64_t n_atoms, const int64_t* __restrict__ rowptr, const void* __restri
 #pragma unroll
       for (int a = 0; a < 3; ++a) {
         const int64_t row = r0 + a;
-        double y = ep.alpha * (double)h[a] + ep.gamma * (double)xs[a];
-        if (ep.has_yin) y += ep.beta * (double)Yin[row * ldyin + c0 + c];
+        double al = ep.alpha, ga = ep.gamma, be = ep.beta;
+        if (ep.seg_coef != nullptr) {
+          const int sg = __ldg(ep.atom_seg + i);
+          al = __ldg(ep.seg_coef + 3 * sg);
+          ga = __ldg(ep.seg_coef + 3 * sg + 1);
+          be = __ldg(ep.seg_coef + 3 * sg + 2);
+        }
+        double y = al * (double)h[a] + ga * (double)xs[a];
+        if (ep.has_yin) y += be * (double)Yin[row * ldyin + c0 + c];
         for (int q = 0; q < ep.r; ++q) y += Q[q * ndof + row] * s_coef[q * B + c];
         Y[row * ldy + c0 + c] = (T)y;
         if (ep.accumulate) Acc[row * ldacc + c0 + c] += (T)(ep.mu * y);
@@ -229,8 +239,15 @@ k_spmm_cols(int64_t n_atoms, const int64_t* __restrict__ rowptr, const void* __r
 #pragma unroll
         for (int a = 0; a < 3; ++a) {
           const int64_t row = r0 + a;
-          double y = ep.alpha * (double)h[a] + ep.gamma * (double)xs[a];
-          if (ep.has_yin) y += ep.beta * (double)Yin[row * ldyin + c0 + c];
+          double al = ep.alpha, ga = ep.gamma, be = ep.beta;
+        if (ep.seg_coef != nullptr) {
+          const int sg = __ldg(ep.atom_seg + i);
+          al = __ldg(ep.seg_coef + 3 * sg);
+          ga = __ldg(ep.seg_coef + 3 * sg + 1);
+          be = __ldg(ep.seg_coef + 3 * sg + 2);
+        }
+        double y = al * (double)h[a] + ga * (double)xs[a];
+          if (ep.has_yin) y += be * (double)Yin[row * ldyin + c0 + c];
           for (int q = 0; q < ep.r; ++q) y += Q[q * ndof + row] * s_coef[q * B + c];
           Y[row * ldy + c0 + c] = (T)y;
           if (ep.accumulate) Acc[row * ldacc + c0 + c] += (T)(ep.mu * y);
@@ -324,8 +341,15 @@ k_spmm_warp(int64_t n_atoms, const int64_t* __restrict__ rowptr, const void* __r
 #pragma unroll
         for (int a = 0; a < 3; ++a) {
           const int64_t row = r0 + a;
-          double y = ep.alpha * (double)h[a] + ep.gamma * (double)xs[a];
-          if (ep.has_yin) y += ep.beta * (double)Yin[row * ldyin + c0 + c];
+          double al = ep.alpha, ga = ep.gamma, be = ep.beta;
+        if (ep.seg_coef != nullptr) {
+          const int sg = __ldg(ep.atom_seg + i);
+          al = __ldg(ep.seg_coef + 3 * sg);
+          ga = __ldg(ep.seg_coef + 3 * sg + 1);
+          be = __ldg(ep.seg_coef + 3 * sg + 2);
+        }
+        double y = al * (double)h[a] + ga * (double)xs[a];
+          if (ep.has_yin) y += be * (double)Yin[row * ldyin + c0 + c];
           for (int q = 0; q < ep.r; ++q) y += Q[q * ndof + row] * s_coef[q * B + c];
           Y[row * ldy + c0 + c] = (T)y;
           if (ep.accumulate) Acc[row * ldacc + c0 + c] += (T)(ep.mu * y);
@@ -608,5 +632,36 @@ extern "C" inch_status inch_spmm_noalloc(int32_t prec, int64_t n_atoms, const in
     err = run<double>(n_atoms, rowptr, ent, diag, X, ldx, b, Y, ldy, Yin, ldyin, Acc, ldacc, ep, q, e.hot_shift,
                       partial, coef, stream);
   INCH_REQUIRE(err == cudaSuccess, INCH_CUDA_ERROR, "inch_spmm_noalloc: %s", cudaGetErrorString(err));
+  return INCH_OK;
+}
+
+// ---------------------------------------------------------------------------
+// Segmented epilogue: block-diagonal stores holding many structures, where each
+// structure (segment) needs its own filter coefficients.
+// ---------------------------------------------------------------------------
+extern "C" inch_status inch_spmm_seg(int32_t prec, int64_t n_atoms, const int64_t* rowptr, const void* ent,
+                                     const void* diag, const void* X, int64_t ldx, int32_t b, void* Y, int64_t ldy,
+                                     const void* Yin, int64_t ldyin, const int32_t* atom_seg,
+                                     const double* seg_coef, cudaStream_t stream) {
+  INCH_REQUIRE(prec == 32 || prec == 64, INCH_INVALID_ARG, "inch_spmm_seg: prec must be 32 or 64");
+  INCH_REQUIRE(rowptr && ent && diag && X && Y && atom_seg && seg_coef, INCH_INVALID_ARG,
+               "inch_spmm_seg: NULL argument");
+  INCH_REQUIRE(n_atoms >= 1 && n_atoms < (int64_t(1) << 31), INCH_INVALID_ARG, "inch_spmm_seg: n_atoms out of range");
+  INCH_REQUIRE(b >= 1 && b <= 64 && ldx >= b && ldy >= b && X != Y, INCH_INVALID_ARG,
+               "inch_spmm_seg: bad b / leading dimension / aliasing");
+  INCH_REQUIRE(Yin == nullptr || ldyin >= b, INCH_INVALID_ARG, "inch_spmm_seg: ldyin below b");
+  INCH_REQUIRE(((uintptr_t)ent & 15) == 0 && ((uintptr_t)diag & 15) == 0, INCH_INVALID_ARG,
+               "inch_spmm_seg: store buffers must be 16-byte aligned");
+  Epi ep{0.0, 0.0, 0.0, 0.0, 0, 0, Yin != nullptr ? 1 : 0};
+  ep.seg_coef = seg_coef;
+  ep.atom_seg = atom_seg;
+  cudaError_t err;
+  if (prec == 32)
+    err = run<float>(n_atoms, rowptr, ent, diag, X, ldx, b, Y, ldy, Yin, ldyin, nullptr, 0, ep, nullptr, 0.0,
+                     nullptr, nullptr, stream);
+  else
+    err = run<double>(n_atoms, rowptr, ent, diag, X, ldx, b, Y, ldy, Yin, ldyin, nullptr, 0, ep, nullptr, 0.0,
+                      nullptr, nullptr, stream);
+  INCH_REQUIRE(err == cudaSuccess, INCH_CUDA_ERROR, "inch_spmm_seg: %s", cudaGetErrorString(err));
   return INCH_OK;
 }

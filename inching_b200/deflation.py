@@ -35,3 +35,40 @@ def rigid_body_basis(X_nm, device=None) -> torch.Tensor:
                 V[:, ix] -= V[:, :ix] @ (V[:, :ix].t() @ V[:, ix])
                 V[:, ix] /= torch.sqrt(V[:, ix] @ V[:, ix])
     return V.t().contiguous()
+
+
+def rigid_body_basis_padded(X_nm: torch.Tensor, atom_offsets, n_max_dof: int) -> torch.Tensor:
+    """Rigid-body bases of many structures at once: X_nm holds the structures'
+    atoms back to back (atom_offsets, S+1); returns (S, 6, n_max_dof) with each
+    structure's six orthonormal rows (same construction as rigid_body_basis,
+    batched over structures; padding is zero)."""
+    dev = X_nm.device
+    off = torch.as_tensor(np.asarray(atom_offsets), device=dev)
+    S = off.numel() - 1
+    sizes = (off[1:] - off[:-1])
+    n_atoms_max = n_max_dof // 3
+    sid = torch.repeat_interleave(torch.arange(S, device=dev), sizes)
+    local = torch.arange(X_nm.shape[0], device=dev) - off[:-1][sid]
+    Xp = torch.zeros((S, n_atoms_max, 3), dtype=torch.float64, device=dev)
+    Xp[sid, local] = X_nm
+    mask = torch.zeros((S, n_atoms_max, 1), dtype=torch.float64, device=dev)
+    mask[sid, local] = 1.0
+    V = torch.zeros((S, 6, n_atoms_max, 3), dtype=torch.float64, device=dev)
+    inv = (1.0 / torch.sqrt(sizes.double()))[:, None]
+    for i in range(3):
+        V[:, i, :, i] = inv * mask[:, :, 0]
+    R = [torch.tensor(m, dtype=torch.float64, device=dev).t() for m in (
+        [[0, 0, 0], [0, 0, -1], [0, 1, 0]], [[0, 0, 1], [0, 0, 0], [-1, 0, 0]], [[0, -1, 0], [1, 0, 0], [0, 0, 0]])]
+    for t in range(3):
+        g = (Xp @ R[t]) * mask
+        V[:, 3 + t] = g / torch.linalg.vector_norm(g.reshape(S, -1), dim=1)[:, None, None]
+    V = V.reshape(S, 6, -1)
+    for _ in range(2):
+        for ix in range(1, 6):
+            for _twice in range(2):
+                c = torch.einsum("srn,sn->sr", V[:, :ix], V[:, ix])
+                V[:, ix] -= torch.einsum("sr,srn->sn", c, V[:, :ix])
+                V[:, ix] /= torch.linalg.vector_norm(V[:, ix], dim=1, keepdim=True)
+    out = torch.zeros((S, 6, n_max_dof), dtype=torch.float64, device=dev)
+    out[:, :, :V.shape[2]] = V
+    return out

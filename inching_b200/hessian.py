@@ -176,6 +176,16 @@ class HessianStore:
             _native.spmm(prec, self.n_atoms, self.rowptr, ent, diag, X[:, sl], out[:, sl], **kw)
         return out
 
+    def matmul_seg(self, X, out, atom_seg, seg_coef, Yin=None, prec=32):
+        """out = alpha_s (H X) + gamma_s X + beta_s Yin with per-segment coefficients
+        (block-diagonal stores of many structures; pair layout)."""
+        ent, diag = self.store(prec)
+        for c0 in range(0, X.shape[1], 64):
+            sl = slice(c0, min(c0 + 64, X.shape[1]))
+            _native.spmm_seg(prec, self.n_atoms, self.rowptr, ent, diag, X[:, sl], out[:, sl], atom_seg, seg_coef,
+                             Yin=None if Yin is None else Yin[:, sl])
+        return out
+
     def __matmul__(self, X):
         return self.matmul(X)
 

@@ -78,21 +78,6 @@ def normal_modes_device(X_nm: torch.Tensor, k: int, *, rc_gamma_A=8.0, plus_i=1.
     return evals - plus_i, modes, info
 
 
-_pinned = {}
-
-
-def _pinned_buffer(shape, dtype):
-    """Reusable page-locked host buffer (allocating 100s of MB of pinned memory
-    per call costs more than the copy itself)."""
-    key = (tuple(shape), dtype)
-    buf = _pinned.get(key)
-    if buf is None:
-        _pinned.clear()
-        buf = torch.empty(shape, dtype=dtype, pin_memory=True)
-        _pinned[key] = buf
-    return buf
-
-
 def normal_modes(X, k: int, *, units="nm", **kw):
     """Host-facing call: X (N,3) numpy in nm (or Angstrom with units="A"); returns
     numpy eigenvalues (k,) (PlusI removed) and eigenvectors (k, N, 3) in the input
@@ -103,6 +88,4 @@ def normal_modes(X, k: int, *, units="nm", **kw):
     Xd = torch.from_numpy(np.ascontiguousarray(Xh)).pin_memory().to("cuda", non_blocking=True)
     evals, modes, info = normal_modes_device(Xd, k, **kw)
     ev = evals.cpu().numpy()
-    out = _pinned_buffer(modes.shape, modes.dtype)
-    out.copy_(modes)
-    return ev, out.numpy().copy(), info
+    return ev, modes.cpu().numpy(), info

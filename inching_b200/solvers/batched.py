@@ -21,7 +21,7 @@ import numpy as np
 import torch
 
 from ..spectrum import estimate_spectrum_bound
-from .chfsi import _Filter
+from .chfsi import _Phases
 
 
 class _Segments:
@@ -56,6 +56,53 @@ class _Segments:
         return P.reshape(self.S * self.n_max, P.shape[2]).index_select(0, self.back)
 
 
+class _FilterSeg:
+    """Scaled Chebyshev filter with each structure's own interval [a_s, b] and
+    normalisation point a0_s; every degree is one segmented SpMM launch (per
+    64-column panel) for all structures of the block-diagonal store."""
+
+    def __init__(self, A, prec, atom_seg):
+        self.A = A
+        self.prec = prec
+        self.atom_seg = atom_seg
+        self.n_spmm = 0
+
+    def __call__(self, X64, m, a, b, a0):
+        a = np.asarray(a, dtype=np.float64)
+        a0 = np.asarray(a0, dtype=np.float64)
+        e = (b - a) / 2.0
+        c = (b + a) / 2.0
+        sigma = e / (a0 - c)
+        sigma1 = sigma.copy()
+        tau = 2.0 / sigma1
+        coefs = [np.stack([sigma1 / e, -sigma1 * c / e, np.zeros_like(e)], axis=1)]
+        for _ in range(2, m + 1):
+            s2 = 1.0 / (tau - sigma)
+            coefs.append(np.stack([2.0 * s2 / e, -2.0 * s2 * c / e, -sigma * s2], axis=1))
+            sigma = s2
+        table = torch.from_numpy(np.ascontiguousarray(np.stack(coefs))).to(X64.device)      # (m, S, 3)
+        dt = torch.float64 if self.prec == 64 else torch.float32
+        nb = X64.shape[1]
+        bp = (nb + 7) // 8 * 8
+        X = torch.zeros((X64.shape[0], bp), dtype=dt, device=X64.device)
+        X[:, :nb] = X64
+        Y = torch.empty_like(X)
+        self.A.matmul_seg(X, Y, self.atom_seg, table[0], prec=self.prec)
+        self.n_spmm += 1
+        for t in range(1, m):
+            self.A.matmul_seg(Y, X, self.atom_seg, table[t], Yin=X, prec=self.prec)
+            X, Y = Y, X
+            self.n_spmm += 1
+        return Y[:, :nb].to(torch.float64)
+
+
+def _eigh_small(G):
+    """Batched symmetric eigensolve of small (S, p, p) matrices on the host
+    (LAPACK): for p of a few dozen this beats the device batched solver by far."""
+    w, V = np.linalg.eigh(G.cpu().numpy())
+    return torch.from_numpy(w).to(G.device), torch.from_numpy(V).to(G.device)
+
+
 def _cholqr_b(P):
     for _ in range(2):
         G = P.transpose(1, 2) @ P
@@ -72,7 +119,7 @@ def _project_b(P, Qp):
 
 
 def chfsi_batched(H, dof_offsets, k, tol=1e-6, Qp=None, precision="mixed", degree=24, guard=None, maxiter=200,
-                  seed=0, verbose=False):
+                  seed=0, verbose=False, profile=False, Y0=None):
     """Lowest k modes (orthogonal to Qp) of every diagonal block of H.
 
     dof_offsets: (S+1,) dof offsets of the structures inside H (block-diagonal).
@@ -80,64 +127,80 @@ def chfsi_batched(H, dof_offsets, k, tol=1e-6, Qp=None, precision="mixed", degre
     Returns (evals (S, k) FP64, vecs (n_total, k) FP64 with each structure's
     rows, info)."""
     dev = H.device
-    seg = _Segments(dof_offsets, dev)
+    ph = _Phases(profile)
+    with ph("segments"):
+        seg = _Segments(dof_offsets, dev)
     S = seg.S
     prec = 32 if precision == "mixed" else 64
     if guard is None:
-        guard = max(12, int(math.ceil(0.3 * k)))
+        guard = max(16, int(math.ceil(0.5 * k)))
     p = min(k + guard, int(seg.sizes.min()) - (0 if Qp is None else Qp.shape[1]))
     assert p > k, "ABORTED. a structure is too small for k modes plus guard vectors"
-    lo, hi = estimate_spectrum_bound(H, steps=40, seed=seed + 1, precision=precision)
+    with ph("bound"):
+        lo, hi = estimate_spectrum_bound(H, steps=40, seed=seed + 1, precision=precision)
     b_up = hi * 1.02 + 1e-3 * abs(hi)
     g = torch.Generator(device=dev)
     g.manual_seed(seed)
     Y = torch.randn((seg.n_total, p), generator=g, dtype=torch.float64, device=dev)
+    if Y0 is not None:
+        c0 = min(Y0.shape[1], p)
+        Y[:, :c0] = Y0[:, :c0]
     P = seg.gather(Y)
     if Qp is not None:
         P = _project_b(P, Qp)
     P = _cholqr_b(P) * seg.mask
-    filt = _Filter(H, prec)
+    atom_sizes = torch.from_numpy(seg.sizes // 3).to(dev)
+    atom_seg = torch.repeat_interleave(torch.arange(S, dtype=torch.int32, device=dev), atom_sizes).contiguous()
+    filt = _FilterSeg(H, prec, atom_seg)
     it = 0
     th = None
     res = None
     for it in range(maxiter):
-        Y = seg.scatter(P)
-        if prec == 64:
-            HY = H.matmul(Y.contiguous(), prec=64)
-        else:
-            HY = H.matmul(Y.to(torch.float32).contiguous(), prec=32).to(torch.float64)
-        HP = seg.gather(HY)
-        G = P.transpose(1, 2) @ HP
-        G = 0.5 * (G + G.transpose(1, 2))
-        th, W = torch.linalg.eigh(G)
-        P = P @ W
-        HP = HP @ W
-        R = HP - P * th[:, None, :]
-        res = torch.linalg.vector_norm(R, dim=1)                      # (S, p)
-        worst = float((res[:, :k] / b_up).max())
+        with ph("rr_spmm"):
+            Y = seg.scatter(P)
+            if prec == 64:
+                HY = H.matmul(Y.contiguous(), prec=64)
+            else:
+                HY = H.matmul(Y.to(torch.float32).contiguous(), prec=32).to(torch.float64)
+            HP = seg.gather(HY)
+        with ph("rr_gemm"):
+            G = P.transpose(1, 2) @ HP
+            G = 0.5 * (G + G.transpose(1, 2))
+        with ph("rr_eigh"):
+            th, W = _eigh_small(G)
+        with ph("rr_rotate"):
+            P = P @ W
+            HP = HP @ W
+            R = HP - P * th[:, None, :]
+            res = torch.linalg.vector_norm(R, dim=1)                      # (S, p)
+            worst = float((res[:, :k] / b_up).max())
         if verbose:
             print(f"batched it {it}: worst rel residual {worst:.2e}")
         if worst <= tol:
             break
-        a = float(th[:, -1].max())
-        a0 = float(th[:, 0].min())
-        if not (a0 < a < b_up):
-            a0 = a - 1e-3 * abs(a)
-        Z = filt(seg.scatter(P), degree, a, b_up, a0 - 1e-12)
-        P = seg.gather(Z)
-        if Qp is not None:
-            P = _project_b(P, Qp)
-        P = _cholqr_b(P) * seg.mask
+        # each structure filters with its own interval: [largest block Ritz value, b]
+        a = th[:, -1].cpu().numpy()
+        a0 = th[:, 0].cpu().numpy()
+        bad = ~((a0 < a) & (a < b_up))
+        a = np.minimum(a, 0.999 * b_up)
+        a0 = np.where(bad, a - 1e-3 * np.abs(a), a0)
+        with ph("filter"):
+            Z = filt(seg.scatter(P), degree, a, b_up, a0 - 1e-12)
+            P = seg.gather(Z)
+        with ph("orth"):
+            if Qp is not None:
+                P = _project_b(P, Qp)
+            P = _cholqr_b(P) * seg.mask
     # final FP64 Rayleigh-Ritz of each structure's block; keep the k lowest
     Y = seg.scatter(P)
     HP = seg.gather(H.matmul(Y.contiguous(), prec=64))
     G = P.transpose(1, 2) @ HP
     G = 0.5 * (G + G.transpose(1, 2))
-    th, W = torch.linalg.eigh(G)
+    th, W = _eigh_small(G)
     thk = th[:, :k].contiguous()
     Pk = P @ W[:, :, :k]
     R = HP @ W[:, :, :k] - Pk * thk[:, None, :]
     rel = torch.linalg.vector_norm(R, dim=1) / b_up
     info = dict(iterations=it + 1, n_spmm_filter=filt.n_spmm, block=p, degree=degree, structures=S,
-                max_rel_residual=float(rel.max()), normH=b_up)
+                max_rel_residual=float(rel.max()), normH=b_up, phases_ms=ph.summary())
     return thk, seg.scatter(Pk), info

@@ -157,6 +157,17 @@ typedef struct {
 } inch_spmm_epilogue;
 
 size_t inch_spmm_workspace_size(int64_t n_atoms, int32_t b, int32_t r);
+/* inch_spmm with per-segment coefficients (no reference counterpart): for a
+ * block-diagonal store holding many structures, atom i uses (alpha, gamma, beta) =
+ * seg_coef[3*atom_seg[i] .. +2] in Y = alpha*(H X) + gamma*X + beta*Yin, so each
+ * structure gets its own Chebyshev filter step in the same launch.  Yin may be
+ * NULL (then beta is ignored) and may alias Y.  No deflation or accumulation. */
+inch_status inch_spmm_seg(int32_t prec, int64_t n_atoms, const int64_t* rowptr_dev,
+                          const void* ent_dev, const void* diag_dev,
+                          const void* X_dev, int64_t ldx, int32_t b,
+                          void* Y_dev, int64_t ldy, const void* Yin_dev, int64_t ldyin,
+                          const int32_t* atom_seg_dev, const double* seg_coef_dev, cudaStream_t stream);
+
 /* Launch shape of the wide-block (b >= 8) SpMM kernel for this process: threads
  * per block (256, 512 or 1024) and resident blocks per SM (1..8); each block walks
  * one contiguous slab of rows.  threads_per_block = 0 selects instead, for tiles of
