@@ -190,10 +190,10 @@ k_spmm_cols(int64_t n_atoms, const int64_t* __restrict__ rowptr, const void* __r
   const int lane = threadIdx.x & 31;
   const int cl = lane % LPR;
   const int grp = (threadIdx.x >> 5) * RPW + lane / LPR;
-  const int64_t per = (n_atoms + gridDim.x - 1) / gridDim.x;
-  const int64_t r_beg = (int64_t)blockIdx.x * per;
-  const int64_t r_end = r_beg + per < n_atoms ? r_beg + per : n_atoms;
-  for (int64_t i = r_beg + grp; i < r_end; i += GPB) {
+  // Block-interleaved rows: at any time the whole grid works on one band of
+  // consecutive rows, so the X_j rows it gathers stay an L2-sized window even
+  // when X itself is many times larger than L2.
+  for (int64_t i = (int64_t)blockIdx.x * GPB + grp; i < n_atoms; i += (int64_t)gridDim.x * GPB) {
     T acc[3][CPL][V];
 #pragma unroll
     for (int t = 0; t < CPL; ++t)

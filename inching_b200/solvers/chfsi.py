@@ -242,3 +242,156 @@ def chfsi(A, k, tol=1e-6, Q=None, precision="mixed", degree=24, guard=None, maxi
                     seconds=time.perf_counter() - t_start, phases_ms=ph.summary())
         return evals_t, L, info
     return evals_t, L
+
+
+# ---------------------------------------------------------------------------
+# Memory-lean variant for structures whose block does not fit several times in HBM
+# ---------------------------------------------------------------------------
+def _rows(n, rows):
+    for r0 in range(0, n, rows):
+        yield slice(r0, min(r0 + rows, n))
+
+
+def chfsi_lean(A, k, tol=1e-6, Q=None, precision="mixed", degree=24, guard=None, maxiter=100, X0=None, seed=0,
+               chunk=256, row_chunk=1 << 20, window=512, verbose=False, return_info=False):
+    """Same iteration as chfsi() with one (n, p) FP64 array B holding the locked
+    modes (columns [0, L)) and the active block (columns [L, p)):
+
+      * the filter runs on column chunks of `chunk` vectors (it acts column by
+        column), with FP32 (or FP64) buffers of that width only;
+      * Rayleigh-Ritz forms G = Y^T H Y chunk by chunk from an FP64 product, so
+        H Y is never stored; explicit FP64 residuals are taken for the leading
+        `window` wanted active columns, the only ones that can lock next;
+      * rotations, projections and Cholesky-QR update B in row chunks;
+      * converged leading active columns become locked by moving L.
+    Peak memory is about n*p*8 bytes plus a few (n, chunk) buffers: the 2.4M-atom,
+    1000-mode configuration (n = 7.2M, p = 1250) needs ~72 GB for B.  A contiguous
+    FP64 X0 of shape (n, p) is used in place as B (it is overwritten)."""
+    t_start = time.perf_counter()
+    n = A.shape[0]
+    dev = A.device
+    prec = 32 if precision == "mixed" else 64
+    if guard is None:
+        guard = default_guard(k)
+    p = min(k + guard, n - (0 if Q is None else Q.shape[0]))
+    Qd = None if Q is None else HessianOperator(A, Q=Q).Q
+    lo, hi = estimate_spectrum_bound(A, steps=40, seed=seed + 1, precision=precision)
+    b_up = hi * 1.02 + 1e-3 * abs(hi)
+    g = torch.Generator(device=dev)
+    g.manual_seed(seed)
+    if (X0 is not None and X0.dtype == torch.float64 and X0.is_contiguous() and tuple(X0.shape) == (n, p)
+            and X0.device == dev):
+        B = X0          # take over the caller's block: no second n x p copy
+    else:
+        B = torch.empty((n, p), dtype=torch.float64, device=dev)
+        c0 = 0 if X0 is None else min(X0.shape[1], p)
+        for cs in range(0, p, chunk):
+            ce = min(cs + chunk, p)
+            if ce <= c0:
+                B[:, cs:ce] = X0[:, cs:ce].to(torch.float64)
+            else:
+                B[:, cs:ce] = torch.randn((n, ce - cs), generator=g, dtype=torch.float64, device=dev)
+                if cs < c0:
+                    B[:, cs:c0] = X0[:, cs:c0].to(torch.float64)
+
+    def project(L):
+        """Active columns minus their components along Q (rigid) and B[:, :L]."""
+        act = slice(L, p)
+        for _ in range(2):
+            for basis in ((Qd.t() if Qd is not None else None), (B[:, :L] if L > 0 else None)):
+                if basis is None:
+                    continue
+                C = basis.t() @ B[:, act]                         # (r, A) small
+                for rs in _rows(n, row_chunk):
+                    B[rs, act] -= basis[rs] @ C
+
+    def orth(L):
+        act = slice(L, p)
+        for _ in range(2):
+            G = B[:, act].t() @ B[:, act]
+            R, info = torch.linalg.cholesky_ex(G, upper=True)
+            if int(info) != 0:
+                raise RuntimeError("chfsi_lean: Gram matrix not positive definite")
+            Rinv = torch.linalg.solve_triangular(R, torch.eye(R.shape[0], dtype=R.dtype, device=dev), upper=True)
+            for rs in _rows(n, row_chunk):
+                B[rs, act] = B[rs, act] @ Rinv
+
+    def rayleigh_ritz(L):
+        """Rotate the active block to Ritz vectors; returns (theta, residual norms).
+        Explicit FP64 residuals are computed for the leading `window` wanted active
+        columns only (locking proceeds from the front); the others report inf."""
+        act_n = p - L
+        G = torch.zeros((act_n, act_n), dtype=torch.float64, device=dev)
+        for cs in range(L, p, chunk):
+            ce = min(cs + chunk, p)
+            HYc = A.matmul(B[:, cs:ce].contiguous(), prec=64)
+            G[:, cs - L:ce - L] = B[:, L:].t() @ HYc
+            del HYc
+        G = 0.5 * (G + G.t())
+        th, W = np.linalg.eigh(G.cpu().numpy())
+        Wd = torch.from_numpy(W).to(dev)
+        for rs in _rows(n, row_chunk):
+            B[rs, L:] = B[rs, L:] @ Wd
+        res = np.full(len(th), np.inf)
+        last = min(len(th), k - L, window)
+        thd = torch.from_numpy(th[:last].copy()).to(dev)
+        for cs in range(0, last, chunk):
+            ce = min(cs + chunk, last)
+            Yc = B[:, L + cs:L + ce].contiguous()
+            R = A.matmul(Yc, prec=64) - Yc * thd[cs:ce][None, :]
+            res[cs:ce] = torch.linalg.vector_norm(R, dim=0).cpu().numpy()
+        return th, res
+
+    project(0)
+    orth(0)
+    th, res = rayleigh_ritz(0)
+    L = 0
+    locked_theta = []
+    filt = _Filter(A, prec)
+    it = 0
+    for it in range(maxiter):
+        nl = 0
+        while L + nl < k and nl < len(th) and res[nl] <= tol * b_up:
+            nl += 1
+        if nl:
+            locked_theta.extend(th[:nl].tolist())
+            th, res = th[nl:], res[nl:]
+            L += nl
+        if verbose:
+            print(f"lean it {it}: locked {L}/{k}, max active res {res[:max(k - L, 1)].max() / b_up:.2e}")
+        if L >= k:
+            break
+        a = float(th[-1])
+        a0 = float(th[0])
+        if not (a0 < a < b_up):
+            a0 = a - 1e-3 * abs(a)
+        for cs in range(L, p, chunk):
+            ce = min(cs + chunk, p)
+            B[:, cs:ce] = filt(B[:, cs:ce], degree, a, b_up, a0 - 1e-12)
+        project(L)
+        orth(L)
+        th, res = rayleigh_ritz(L)
+    converged = L >= k
+    # final FP64 Rayleigh-Ritz over the first k columns, explicit residuals
+    Lk = B[:, :k]
+    G = torch.zeros((k, k), dtype=torch.float64, device=dev)
+    for cs in range(0, k, chunk):
+        ce = min(cs + chunk, k)
+        G[:, cs:ce] = Lk.t() @ A.matmul(Lk[:, cs:ce].contiguous(), prec=64)
+    G = 0.5 * (G + G.t())
+    thf, W = np.linalg.eigh(G.cpu().numpy())
+    Wd = torch.from_numpy(W).to(dev)
+    for rs in _rows(n, row_chunk):
+        B[rs, :k] = B[rs, :k] @ Wd
+    thd = torch.from_numpy(thf).to(dev)
+    worst = 0.0
+    for cs in range(0, k, chunk):
+        ce = min(cs + chunk, k)
+        R = A.matmul(B[:, cs:ce].contiguous(), prec=64) - B[:, cs:ce] * thd[cs:ce][None, :]
+        worst = max(worst, float(torch.linalg.vector_norm(R, dim=0).max()) / b_up)
+    evals = torch.from_numpy(thf.copy()).to(dev)
+    V = B[:, :k]
+    if return_info:
+        return evals, V, dict(iterations=it + 1, converged=converged, n_spmm_filter=filt.n_spmm, block=p,
+                              degree=degree, normH=b_up, max_rel_residual=worst, seconds=time.perf_counter() - t_start)
+    return evals, V

@@ -45,7 +45,10 @@ def coarse_warm_start(X_nm: torch.Tensor, n_vectors: int, bead_edge_A=6.0, rc_be
     Qc = rigid_body_basis(pos)
     ev, Vc, info = chfsi(Hc, m, tol=tol, Q=Qc, precision="mixed", seed=seed + 7, return_info=True)
     Vb = Vc.reshape(nb, 3, m)
+    del Vc, Hc
     V = Vb.index_select(0, bead).reshape(3 * X_nm.shape[0], m)
+    if m < n_vectors:      # pad with random columns so the block has the requested width
+        V = torch.cat([V, torch.randn((V.shape[0], n_vectors - m), dtype=V.dtype, device=V.device)], dim=1)
     if return_info:
         return V, dict(beads=int(nb), coarse_modes=m, coarse_iterations=info["iterations"],
                        coarse_seconds=info["seconds"])

@@ -166,3 +166,17 @@ def test_pipeline_undo_order_and_rigid_orthogonality():
     v1 = modes[0].ravel()
     v2 = modes2[0][np.argsort(perm)].ravel()
     assert abs(abs(v1 @ v2) - 1.0) < 1e-6
+
+
+@pytest.mark.parametrize("precision,tol,eig_tol,ang_tol", [("f64", 1e-9, 1e-10, 1e-4), ("mixed", 1e-6, 1e-6, 1e-2)])
+def test_chfsi_lean_matches_dense(small, precision, tol, eig_tol, ang_tol):
+    """Memory-lean block solver (column-chunked filter and Rayleigh-Ritz, row-chunked
+    updates, locked modes kept in the same array) vs dense LAPACK."""
+    from inching_b200.solvers.chfsi import chfsi_lean
+    s = small
+    S, V, info = chfsi_lean(s["H"], 40, tol=tol, Q=s["Q"], precision=precision, chunk=16, row_chunk=1000,
+                            window=24, return_info=True)
+    ref = s["w"][6:46]
+    assert info["converged"] and info["max_rel_residual"] <= 1.5 * tol
+    assert np.max(np.abs(S.cpu().numpy() - ref) / ref) < eig_tol
+    assert max_cluster_angle(V.cpu().numpy(), s["U"], s["w"], 6, 46) < ang_tol
