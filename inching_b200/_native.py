@@ -81,6 +81,24 @@ _SIGS = {
     "inch_spmm_tiles": (ctypes.c_int, [c_int32, c_int64, c_void_p, c_void_p, c_void_p, c_void_p, c_void_p,
                                        c_void_p, c_int64, c_int32, c_void_p, c_int64, c_void_p, c_int64, c_void_p,
                                        c_int64, c_void_p, POINTER(SpmmEpilogue), c_void_p, c_size_t, c_void_p]),
+    "inch_hessian_assemble_weighted": (ctypes.c_int, [c_void_p, c_int64, c_double, c_double, c_void_p, c_void_p,
+                                                      c_void_p, c_void_p, c_void_p, c_void_p, c_void_p, c_void_p]),
+    "inch_mp_edge_concat": (ctypes.c_int, [c_void_p, c_void_p, c_void_p, c_int64, c_int32, c_int32, c_void_p,
+                                           c_void_p]),
+    "inch_mp_edge_concat_bwd": (ctypes.c_int, [c_void_p, c_void_p, c_int64, c_int32, c_int32, c_void_p, c_void_p]),
+    "inch_mp_segment_sum": (ctypes.c_int, [c_void_p, c_void_p, c_int64, c_int32, c_void_p, c_void_p]),
+    "inch_mp_segment_sum_bwd": (ctypes.c_int, [c_void_p, c_void_p, c_void_p, c_int64, c_int32, c_void_p, c_void_p]),
+    "inch_mp_bias_relu": (ctypes.c_int, [c_void_p, c_void_p, c_int64, c_int32, c_void_p]),
+    "inch_mp_relu_bwd": (ctypes.c_int, [c_void_p, c_void_p, c_int64, c_void_p]),
+    "inch_mp_edge_pair": (ctypes.c_int, [c_void_p, c_void_p, c_void_p, c_void_p, c_int64, c_int32, c_int32,
+                                         c_void_p, c_void_p]),
+    "inch_mp_edge_pair_bwd": (ctypes.c_int, [c_void_p, c_void_p, c_void_p, c_int64, c_int32, c_int32, c_void_p,
+                                             c_void_p]),
+    "inch_mp_softplus": (ctypes.c_int, [c_void_p, c_int64, ctypes.c_float, c_void_p, c_void_p, c_void_p, c_void_p]),
+    "inch_mp_hf_grad": (ctypes.c_int, [c_void_p, c_void_p, c_void_p, c_void_p, c_void_p, c_int32, c_void_p,
+                                       c_int64, c_void_p, c_void_p]),
+    "inch_mp_adam": (ctypes.c_int, [c_void_p, c_void_p, c_void_p, c_void_p, c_int64, ctypes.c_float,
+                                    ctypes.c_float, ctypes.c_float, ctypes.c_float, c_int32, c_void_p]),
     "inch_spmm_noalloc": (ctypes.c_int, [c_int32, c_int64, c_void_p, c_void_p, c_void_p, c_void_p, c_int64,
                                          c_int32, c_void_p, c_int64, c_void_p, c_int64, c_void_p, c_int64,
                                          c_void_p, POINTER(SpmmEpilogue), c_void_p]),
@@ -204,7 +222,7 @@ def band_slices(rowptr, cols, n_atoms, heads, gap=100, max_slices=256):
 # ---------------------------------------------------------------------------
 # Hessian store and operator
 # ---------------------------------------------------------------------------
-def hessian_assemble(X, rowptr, cols, rc_nm, plus_i, want64=True, want32=True):
+def hessian_assemble(X, rowptr, cols, rc_nm, plus_i, want64=True, want32=True, pair_weight=None):
     _require_cuda(X, "X", torch.float64)
     _require_cuda(rowptr, "rowptr", torch.int64)
     _require_cuda(cols, "cols", torch.int32)
@@ -215,8 +233,14 @@ def hessian_assemble(X, rowptr, cols, rc_nm, plus_i, want64=True, want32=True):
     diag64 = torch.empty((n, 8), dtype=torch.float64, device=dev) if want64 else None
     ent32 = torch.empty((nnz, 4), dtype=torch.float32, device=dev) if want32 else None
     diag32 = torch.empty((n, 8), dtype=torch.float32, device=dev) if want32 else None
-    check(lib().inch_hessian_assemble(_ptr(X), n, rc_nm, plus_i, _ptr(rowptr), _ptr(cols), _ptr(ent64),
-                                      _ptr(diag64), _ptr(ent32), _ptr(diag32), _stream()))
+    if pair_weight is None:
+        check(lib().inch_hessian_assemble(_ptr(X), n, rc_nm, plus_i, _ptr(rowptr), _ptr(cols), _ptr(ent64),
+                                          _ptr(diag64), _ptr(ent32), _ptr(diag32), _stream()))
+    else:
+        _require_cuda(pair_weight, "pair_weight", torch.float64)
+        check(lib().inch_hessian_assemble_weighted(_ptr(X), n, rc_nm, plus_i, _ptr(rowptr), _ptr(cols),
+                                                   _ptr(pair_weight), _ptr(ent64), _ptr(diag64), _ptr(ent32),
+                                                   _ptr(diag32), _stream()))
     _count(1)
     return ent64, diag64, ent32, diag32
 
@@ -335,3 +359,13 @@ def spmm_tiles(prec, n_atoms, uptr, pptr, urec, pw, diag, X, Y, *, alpha=1.0, ga
             tiles += 1
     _count(tiles * (3 if r > 0 else 1))
     return Y
+
+
+# ---------------------------------------------------------------------------
+# Message-passing network kernels (learned warm start)
+# ---------------------------------------------------------------------------
+def mp(name, *args):
+    """Call inch_mp_<name>(*args, stream): tensors become device pointers."""
+    conv = [(_ptr(a) if isinstance(a, torch.Tensor) else a) for a in args]
+    check(getattr(lib(), "inch_mp_" + name)(*conv, _stream()))
+    _count(1)

@@ -17,7 +17,7 @@ constexpr int kWarps = 8;
 __global__ void __launch_bounds__(kWarps * 32)
 k_assemble(const double* __restrict__ X, int64_t n, double r2, double plus_i, const int64_t* __restrict__ rowptr,
            const int* __restrict__ cols, double2* __restrict__ ent64, double* __restrict__ diag64,
-           float4* __restrict__ ent32, float* __restrict__ diag32) {
+           float4* __restrict__ ent32, float* __restrict__ diag32, const double* __restrict__ pair_w) {
   const int lane = threadIdx.x & 31;
   for (int64_t i = (int64_t)blockIdx.x * kWarps + (threadIdx.x >> 5); i < n; i += (int64_t)gridDim.x * kWarps) {
     const double xi = X[3 * i], yi = X[3 * i + 1], zi = X[3 * i + 2];
@@ -28,7 +28,8 @@ k_assemble(const double* __restrict__ X, int64_t n, double r2, double plus_i, co
       // Same rounding as the neighbour test, so the pair set matches the adjacency.
       const double d2 = __dadd_rn(__dadd_rn(__dmul_rn(dx, dx), __dmul_rn(dy, dy)), __dmul_rn(dz, dz));
       const bool ok = d2 > 0.0 && d2 <= r2;
-      const double inv = ok ? 1.0 / sqrt(d2) : 0.0;
+      double inv = ok ? 1.0 / sqrt(d2) : 0.0;
+      if (pair_w != nullptr) inv *= sqrt(pair_w[e]);   // spring constant gamma_e: block = -gamma u u^T
       const double wx = dx * inv, wy = dy * inv, wz = dz * inv;
       s[0] += wx * wx;
       s[1] += wy * wy;
@@ -72,7 +73,25 @@ extern "C" inch_status inch_hessian_assemble(const double* X, int64_t n, double 
   const int g = grid_for(n, kWarps, 148 * 16);
   k_assemble<<<g, kWarps * 32, 0, stream>>>(X, n, rc * rc, plus_i, rowptr, cols,
                                              reinterpret_cast<double2*>(ent64), diag64,
-                                             reinterpret_cast<float4*>(ent32), diag32);
+                                             reinterpret_cast<float4*>(ent32), diag32, nullptr);
+  INCH_LAUNCH_CHECK();
+  return INCH_OK;
+}
+
+extern "C" inch_status inch_hessian_assemble_weighted(const double* X, int64_t n, double rc, double plus_i,
+                                                      const int64_t* rowptr, const int32_t* cols,
+                                                      const double* pair_weight, double* ent64, double* diag64,
+                                                      float* ent32, float* diag32, cudaStream_t stream) {
+  INCH_REQUIRE(X && rowptr && cols && pair_weight, INCH_INVALID_ARG, "inch_hessian_assemble_weighted: NULL argument");
+  INCH_REQUIRE(n >= 1 && n < (int64_t(1) << 31), INCH_INVALID_ARG, "inch_hessian_assemble_weighted: bad n_atoms");
+  INCH_REQUIRE((ent64 != nullptr) == (diag64 != nullptr) && (ent32 != nullptr) == (diag32 != nullptr) &&
+                   (ent64 || ent32),
+               INCH_INVALID_ARG, "inch_hessian_assemble_weighted: bad outputs");
+  INCH_REQUIRE((reinterpret_cast<uintptr_t>(ent64) & 15) == 0 && (reinterpret_cast<uintptr_t>(ent32) & 15) == 0,
+               INCH_INVALID_ARG, "inch_hessian_assemble_weighted: entry buffers must be 16-byte aligned");
+  const int g = grid_for(n, kWarps, 148 * 16);
+  k_assemble<<<g, kWarps * 32, 0, stream>>>(X, n, rc * rc, plus_i, rowptr, cols, reinterpret_cast<double2*>(ent64),
+                                             diag64, reinterpret_cast<float4*>(ent32), diag32, pair_weight);
   INCH_LAUNCH_CHECK();
   return INCH_OK;
 }

@@ -50,7 +50,7 @@ class HessianStore:
     order the caller wants (normally reversed Cuthill-McKee)."""
 
     def __init__(self, X_nm, rc_gamma_A: float = 8.0, plus_i: float = 1.0, precisions=("f64", "f32"),
-                 device=None, graph_=None, tiles=False):
+                 device=None, graph_=None, tiles=False, pair_weight=None):
         self.X = graph.to_device_coords(X_nm, device)
         self.device = self.X.device
         self.n_atoms = int(self.X.shape[0])
@@ -62,7 +62,7 @@ class HessianStore:
         want64 = "f64" in precisions
         want32 = "f32" in precisions
         self.ent64, self.diag64, self.ent32, self.diag32 = _native.hessian_assemble(
-            self.X, self.rowptr, self.cols, self.rc_nm, self.plus_i, want64, want32)
+            self.X, self.rowptr, self.cols, self.rc_nm, self.plus_i, want64, want32, pair_weight=pair_weight)
         n = 3 * self.n_atoms
         self.shape = (n, n)
         self.ndim = 2

@@ -48,7 +48,10 @@ def normal_modes_device(X_nm: torch.Tensor, k: int, *, rc_gamma_A=8.0, plus_i=1.
     """Lowest k non-rigid modes of the structure X_nm (CUDA (N,3) float64, nm).
 
     warm_start="coarse" (block solver only): initial block from the lowest modes
-    of a bead model of the structure (inching_b200.warmstart).
+    of a bead model of the structure (inching_b200.warmstart); "learned": the bead
+    model's spring constants set by the trained network (inching_b200.learned;
+    warm_model= a WarmStartMPNN, default the shipped weights), with its residual
+    test and random-start fallback.
 
     tol: for "chfsi", the relative residual ||Hv - lambda v|| <= tol*||H||; for the
     reference solvers, their own absolute tolerance.  Returns (eigval (k,) with
@@ -66,6 +69,14 @@ def normal_modes_device(X_nm: torch.Tensor, k: int, *, rc_gamma_A=8.0, plus_i=1.
         from .warmstart import coarse_warm_start
         from .solvers.chfsi import default_guard
         kw["X0"], winfo = coarse_warm_start(Xr, k + default_guard(k), seed=seed, return_info=True)
+    elif warm_start == "learned":
+        if solver != "chfsi":
+            raise AssertionError("ABORTED. warm_start='learned' is available for solver='chfsi'")
+        from .learned import WarmStartMPNN, learned_warm_start
+        from .solvers.chfsi import default_guard
+        kw["X0"], winfo = learned_warm_start(Xr, k + default_guard(k), kw.pop("warm_model", None) or
+                                             WarmStartMPNN.load(device=X_nm.device), H.rowptr, H.cols,
+                                             H=H, Q=Q, k=k, seed=seed, return_info=True)
     elif warm_start is not None:
         raise AssertionError(f"ABORTED. unknown warm_start {warm_start!r}")
     t1 = time.perf_counter()

@@ -17,7 +17,10 @@ projection a tall-skinny GEMM:
                        modes (FP64 GEMMs)
   Y <- orth(Y)         Cholesky-QR twice (FP64)
   Rayleigh-Ritz        G = Y^T H Y, eigh (FP64), rotate; residuals ||H y - theta y||
-  lock                 leading Ritz pairs with residual <= tol * ||H||
+  lock                 leading Ritz pairs with residual <= tol * ||H||; after
+                       STALL_RESTART iterations without a new lock, one
+                       Rayleigh-Ritz over locked + active vectors and locking
+                       starts again (see the loop)
 
 precision="mixed": filter and in-loop Rayleigh-Ritz products on the FP32 store
 with FP32 blocks; projections, orthonormalisation, the small eigenproblems and
@@ -34,6 +37,9 @@ import torch
 
 from ..krylov import HessianOperator
 from ..spectrum import estimate_spectrum_bound
+
+
+STALL_RESTART = 3    # iterations without a new lock before the locked + active Rayleigh-Ritz
 
 
 def default_guard(k):
@@ -98,6 +104,73 @@ class _Filter:
         return Y[:, :b].to(torch.float64)
 
 
+class _GraphFilter:
+    """The scaled Chebyshev filter of _Filter, captured as one CUDA graph per block
+    width: its m SpMM launches read their coefficients from a device table (the
+    segmented epilogue with a single segment), so a new filter interval only
+    rewrites that table and the whole filter replays as one graph launch."""
+
+    def __init__(self, A, prec):
+        self.A = A
+        self.prec = prec
+        self.n_spmm = 0
+        self.graphs = {}
+        self.seg = torch.zeros(A.n_atoms, dtype=torch.int32, device=A.device)
+        self.replays = 0
+
+    def _build(self, bp, m):
+        dt = torch.float64 if self.prec == 64 else torch.float32
+        n = self.A.shape[0]
+        X = torch.zeros((n, bp), dtype=dt, device=self.A.device)
+        Y = torch.zeros_like(X)
+        table = torch.zeros((m, 1, 3), dtype=torch.float64, device=self.A.device)
+        out = {"X": X, "Y": Y, "table": table}
+
+        def body():
+            x, y = X, Y
+            self.A.matmul_seg(x, y, self.seg, table[0], prec=self.prec)
+            for t in range(1, m):
+                self.A.matmul_seg(y, x, self.seg, table[t], Yin=x, prec=self.prec)
+                x, y = y, x
+            out["res"] = y
+
+        s = torch.cuda.Stream()
+        s.wait_stream(torch.cuda.current_stream())
+        with torch.cuda.stream(s):
+            body()                                  # warm-up outside capture
+        torch.cuda.current_stream().wait_stream(s)
+        g = torch.cuda.CUDAGraph()
+        with torch.cuda.graph(g):
+            body()
+        out["graph"] = g
+        return out
+
+    def __call__(self, X64, m, a, b, a0):
+        nb = X64.shape[1]
+        bp = (nb + 7) // 8 * 8
+        key = (bp, m)
+        if key not in self.graphs:
+            self.graphs[key] = self._build(bp, m)
+        gph = self.graphs[key]
+        e = (b - a) / 2.0
+        c = (b + a) / 2.0
+        sigma = e / (a0 - c)
+        sigma1 = sigma
+        tau = 2.0 / sigma1
+        rows = [[sigma1 / e, -sigma1 * c / e, 0.0]]
+        for _ in range(2, m + 1):
+            s2 = 1.0 / (tau - sigma)
+            rows.append([2.0 * s2 / e, -2.0 * s2 * c / e, -sigma * s2])
+            sigma = s2
+        gph["table"].copy_(torch.tensor(rows, dtype=torch.float64).reshape(m, 1, 3))
+        gph["X"].zero_()
+        gph["X"][:, :nb] = X64
+        gph["graph"].replay()
+        self.n_spmm += m
+        self.replays += 1
+        return gph["res"][:, :nb].to(torch.float64)
+
+
 def _rr(A, Y, prec):
     """Rayleigh-Ritz on orthonormal Y (n, p): returns theta (asc, numpy), Y W, (H Y) W."""
     if prec == 64:
@@ -145,7 +218,7 @@ class _Span:
 
 
 def chfsi(A, k, tol=1e-6, Q=None, precision="mixed", degree=24, guard=None, maxiter=300, X0=None, seed=0,
-          spectrum_upper=None, final_f64=True, verbose=False, return_info=False, profile=False):
+          spectrum_upper=None, final_f64=True, verbose=False, return_info=False, profile=False, cuda_graph=False):
     """Lowest k eigenpairs of A (+PlusI) orthogonal to the rows of Q.
 
     tol is relative: a pair is locked when ||H y - theta y|| <= tol * ||H||, with
@@ -179,11 +252,13 @@ def chfsi(A, k, tol=1e-6, Q=None, precision="mixed", degree=24, guard=None, maxi
         Y = _cholqr(_project_out(Y, Qd))
     with ph("rr"):
         th, Y, HY = _rr(A, Y, prec)
-    filt = _Filter(A, prec)
+    filt = _GraphFilter(A, prec) if (cuda_graph and hasattr(A, "matmul_seg")) else _Filter(A, prec)
     locked = torch.empty((0, n), dtype=torch.float64, device=dev)   # rows
     locked_theta = []
     it = 0
     n_rr = 1
+    n_restarts = 0
+    stall = 0
     res = np.full(p, np.inf)
     for it in range(maxiter):
         with ph("residual"):
@@ -202,6 +277,21 @@ def chfsi(A, k, tol=1e-6, Q=None, precision="mixed", degree=24, guard=None, maxi
                   f"{res[nl:want].max() / normH if want > nl else 0:.2e} a={th[-1]:.4f}")
         if locked.shape[0] >= k:
             break
+        stall = 0 if nl else stall + 1
+        if stall >= STALL_RESTART and locked.shape[0]:
+            # A locked vector is only accurate to tol; inside a cluster whose gaps are
+            # of the order of tol*||H|| it carries a sizeable share of unlocked
+            # neighbours, and the active block (kept orthogonal to it) cannot get
+            # below tol.  One Rayleigh-Ritz over locked + active resolves that
+            # coupling; locking then starts again from the new Ritz pairs.
+            with ph("rr"):
+                th, Y, HY = _rr(A, torch.cat([locked.t(), Y], dim=1), prec)
+            locked = locked[:0]
+            locked_theta = []
+            n_rr += 1
+            n_restarts += 1
+            stall = 0
+            continue
         a = float(th[-1])
         a0 = float(min(th[0], locked_theta[0] if locked_theta else th[0]))
         if not (a0 < a < b_up):
@@ -237,6 +327,7 @@ def chfsi(A, k, tol=1e-6, Q=None, precision="mixed", degree=24, guard=None, maxi
     evals_t = torch.from_numpy(np.ascontiguousarray(evals)).to(dev)
     if return_info:
         info = dict(iterations=it + 1, converged=converged, n_spmm_filter=filt.n_spmm, n_rr=n_rr,
+                    filter_graph_replays=getattr(filt, "replays", 0), lock_restarts=n_restarts,
                     normH=normH, degree=degree, block=p,
                     max_rel_residual=None if final_res is None else float(final_res.max()),
                     seconds=time.perf_counter() - t_start, phases_ms=ph.summary())
@@ -349,6 +440,8 @@ def chfsi_lean(A, k, tol=1e-6, Q=None, precision="mixed", degree=24, guard=None,
     locked_theta = []
     filt = _Filter(A, prec)
     it = 0
+    stall = 0
+    n_restarts = 0
     for it in range(maxiter):
         nl = 0
         while L + nl < k and nl < len(th) and res[nl] <= tol * b_up:
@@ -361,6 +454,16 @@ def chfsi_lean(A, k, tol=1e-6, Q=None, precision="mixed", degree=24, guard=None,
             print(f"lean it {it}: locked {L}/{k}, max active res {res[:max(k - L, 1)].max() / b_up:.2e}")
         if L >= k:
             break
+        stall = 0 if nl else stall + 1
+        if stall >= STALL_RESTART and L:
+            # locked + active Rayleigh-Ritz, as in chfsi(): clears the coupling of
+            # the active block to modes locked inside a tight cluster
+            th, res = rayleigh_ritz(0)
+            L = 0
+            locked_theta = []
+            stall = 0
+            n_restarts += 1
+            continue
         a = float(th[-1])
         a0 = float(th[0])
         if not (a0 < a < b_up):
@@ -393,5 +496,6 @@ def chfsi_lean(A, k, tol=1e-6, Q=None, precision="mixed", degree=24, guard=None,
     V = B[:, :k]
     if return_info:
         return evals, V, dict(iterations=it + 1, converged=converged, n_spmm_filter=filt.n_spmm, block=p,
-                              degree=degree, normH=b_up, max_rel_residual=worst, seconds=time.perf_counter() - t_start)
+                              degree=degree, normH=b_up, max_rel_residual=worst, lock_restarts=n_restarts,
+                              seconds=time.perf_counter() - t_start)
     return evals, V

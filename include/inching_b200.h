@@ -141,6 +141,51 @@ inch_status inch_hessian_assemble(const double* X_dev, int64_t n_atoms, double r
                                   double* ent64_dev, double* diag64_dev,
                                   float* ent32_dev, float* diag32_dev, cudaStream_t stream);
 
+/* As inch_hessian_assemble with a spring constant per adjacency entry
+ * (pair_weight_dev[e] >= 0, the same value for both directions of a pair): block
+ * (i,j) = -gamma_e u u^T, stored as w = sqrt(gamma_e) u.  Used by the learned
+ * bead model of the warm start; no reference counterpart (the reference's
+ * gamma is 1). */
+inch_status inch_hessian_assemble_weighted(const double* X_dev, int64_t n_atoms, double rc, double plus_i,
+                                           const int64_t* rowptr_dev, const int32_t* cols_dev,
+                                           const double* pair_weight_dev, double* ent64_dev, double* diag64_dev,
+                                           float* ent32_dev, float* diag32_dev, cudaStream_t stream);
+
+/* ---------------------------------------------------------------------------
+ * Message-passing network kernels of the learned warm start (no reference
+ * counterpart).  Directed bead-graph edges in CSR by destination: rowptr (N+1),
+ * src[e] / dst[e] per edge.  Dense layers are GEMMs done by the caller.
+ *   edge_concat      Z[e] = [H[src[e]], EF[e]]           (+ bwd: scatter-add)
+ *   segment_sum      M[i] = mean of A over the edges of row i (+ bwd: gather / deg)
+ *   bias_relu        Y = relu(Y + b);  relu_bwd  dY *= (Y > 0)
+ *   edge_pair        R[e] = [H[dst] + H[src], EF[e]]     (+ bwd)
+ *   softplus         gamma = softplus(s) + floor, or ds = sigmoid(s) * dgamma
+ *   hf_grad          out[e] = 1/2 sum_t c[t] (u_e . (V_t[a] - V_t[b]))^2
+ *                    (Hellmann-Feynman eigenvalue gradient of the bead Hessian)
+ *   adam             one bias-corrected Adam step
+ * ------------------------------------------------------------------------- */
+inch_status inch_mp_edge_concat(const float* H, const float* EF, const int32_t* src, int64_t E, int32_t F,
+                                int32_t G, float* Z, cudaStream_t stream);
+inch_status inch_mp_edge_concat_bwd(const float* dZ, const int32_t* src, int64_t E, int32_t F, int32_t G,
+                                    float* dH, cudaStream_t stream);
+inch_status inch_mp_segment_sum(const float* A, const int64_t* rowptr, int64_t N, int32_t F, float* M,
+                                cudaStream_t stream);
+inch_status inch_mp_segment_sum_bwd(const float* dM, const int64_t* rowptr, const int32_t* dst, int64_t E,
+                                    int32_t F, float* dA, cudaStream_t stream);
+inch_status inch_mp_bias_relu(float* Y, const float* b, int64_t R, int32_t F, cudaStream_t stream);
+inch_status inch_mp_relu_bwd(float* dY, const float* Y, int64_t n, cudaStream_t stream);
+inch_status inch_mp_edge_pair(const float* H, const float* EF, const int32_t* src, const int32_t* dst, int64_t E,
+                              int32_t F, int32_t G, float* R, cudaStream_t stream);
+inch_status inch_mp_edge_pair_bwd(const float* dR, const int32_t* src, const int32_t* dst, int64_t E, int32_t F,
+                                  int32_t G, float* dH, cudaStream_t stream);
+inch_status inch_mp_softplus(const float* s, int64_t E, float floor_v, double* gamma, const double* dgamma,
+                             float* ds, cudaStream_t stream);
+inch_status inch_mp_hf_grad(const double* P, const int64_t* rowptr, const int32_t* src, const int32_t* dst,
+                            const double* V, int32_t m, const double* c, int64_t E, double* out,
+                            cudaStream_t stream);
+inch_status inch_mp_adam(float* w, const float* g, float* m1, float* m2, int64_t n, float lr, float b1, float b2,
+                         float eps, int32_t step, cudaStream_t stream);
+
 /* ---------------------------------------------------------------------------
  * Hessian x multivector with fused epilogue.  X and Y are (3N, b) row-major with
  * leading dimension ld (>= b), element (dof, c) at dof*ld + c.
