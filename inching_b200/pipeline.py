@@ -6,7 +6,7 @@ Mirrors the benchmark drivers (Command8A/commandBenchmark_InchingTRLMHD_Linux_Pd
   2. reversed Cuthill-McKee order                     (X_KdCuthillMckeeOrder)
   3. Hessian H + PlusI*I of the reordered structure   (ReturnCupyHLowerTriangle)
   4. six rigid-body vectors for explicit deflation    (driver lines 314-372)
-  5. eigensolver (TRLM / JDM / IRLM / block ChFSI)
+  5. eigensolver (TRLM / JDM / IRLM / CDM / block ChFSI)
   6. eigenvalues - PlusI, eigenvectors reshaped (k, N, 3) and put back in the
      caller's atom order                               (driver lines 396-407)
 Everything from step 2 on runs on the GPU; `normal_modes` takes and returns host
@@ -23,7 +23,7 @@ from . import graph
 from .deflation import rigid_body_basis
 from .hessian import HessianStore
 
-SOLVERS = ("chfsi", "trlm", "jdm", "irlm")
+SOLVERS = ("chfsi", "trlm", "jdm", "irlm", "cdm")
 
 
 def _solve(H, k, solver, precision, tol, Q, shift, seed, **kw):
@@ -39,6 +39,12 @@ def _solve(H, k, solver, precision, tol, Q, shift, seed, **kw):
     if solver == "irlm":
         from .solvers.irlm import irlm
         return irlm(H, k=k, tol=tol, Q=Q, shift=shift, precision=precision, seed=seed, return_info=True, **kw)
+    if solver == "cdm":
+        from .solvers.cdm import cdm
+        from .spectrum import estimate_spectrum_bound
+        bound = kw.pop("spectrum_bound", None) or estimate_spectrum_bound(H, steps=300, seed=seed + 1)
+        return cdm(H, k=k, tol=tol, Q=Q, precision=precision, spectrum_bound=bound, seed=seed, return_info=True,
+                   **kw)
     raise AssertionError(f"ABORTED. unknown solver {solver!r}; use one of {SOLVERS}")
 
 

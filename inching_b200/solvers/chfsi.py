@@ -146,12 +146,6 @@ class _GraphFilter:
         return out
 
     def __call__(self, X64, m, a, b, a0):
-        nb = X64.shape[1]
-        bp = (nb + 7) // 8 * 8
-        key = (bp, m)
-        if key not in self.graphs:
-            self.graphs[key] = self._build(bp, m)
-        gph = self.graphs[key]
         e = (b - a) / 2.0
         c = (b + a) / 2.0
         sigma = e / (a0 - c)
@@ -162,6 +156,18 @@ class _GraphFilter:
             s2 = 1.0 / (tau - sigma)
             rows.append([2.0 * s2 / e, -2.0 * s2 * c / e, -sigma * s2])
             sigma = s2
+        return self.run_rows(X64, rows)
+
+    def run_rows(self, X64, rows):
+        """Any three-term recurrence X_1 = a_0 H X_0 + g_0 X_0,
+        X_{t+1} = a_t H X_t + g_t X_t + b_t X_{t-1}; rows[t] = (a_t, g_t, b_t)."""
+        m = len(rows)
+        nb = X64.shape[1]
+        bp = (nb + 7) // 8 * 8
+        key = (bp, m)
+        if key not in self.graphs:
+            self.graphs[key] = self._build(bp, m)
+        gph = self.graphs[key]
         gph["table"].copy_(torch.tensor(rows, dtype=torch.float64).reshape(m, 1, 3))
         gph["X"].zero_()
         gph["X"][:, :nb] = X64

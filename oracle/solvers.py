@@ -1,5 +1,6 @@
 """Oracle eigensolvers: numpy restatements of the reference's TRLM, JDM (with
-its projected GMRES), IRLM, Chebyshev filter application and spectrum bound.
+its projected GMRES), IRLM, Chebyshev-Davidson (CDM), Chebyshev filter
+application and spectrum bound.
 
 TEST INFRASTRUCTURE ONLY (see oracle/__init__.py).  Every solver takes a
 callable ``op(v) -> H v`` for the (+PlusI) Hessian so it can run on the scipy
@@ -273,3 +274,90 @@ def jdm(op, n, k=16, tol=1e-10, maxiter=1000, correction_maxiter=20, workspace_f
 def ritz_residuals(op, lam, vecs):
     """||H v - lambda v||_2 per column."""
     return np.array([np.linalg.norm(op(vecs[:, i]) - lam[i] * vecs[:, i]) for i in range(len(lam))])
+
+
+# ---------------------------------------------------------------------------
+# Chebyshev-Davidson, Burn/ChebyshevDavidsonSubspaceIteration/T1.py:229-623
+# ---------------------------------------------------------------------------
+def cdm_filter(op, x, degree, low, high):
+    """Unscaled Chebyshev filter T_{degree+1}((c - H)/e) x on [low, high]
+    (T1.py:195-226): y = (c x - H x)/e, then degree times y' = 2 (c y - H y)/e - x."""
+    e = (high - low) / 2.0
+    c = (high + low) / 2.0
+    z = x.copy()
+    y = (c * z - op(z)) / e
+    for _ in range(degree):
+        ynew = 2.0 * (c * y - op(y)) / e - z
+        z, y = y, ynew
+    return y
+
+
+def cdm(op, n, k=16, tol=1e-10, maxiter=100000, workspace_factor=2, degree=80, spectrum_bound=None, seed=0):
+    """Single-vector Chebyshev-Davidson as in T1.py:229-623: one filtered vector
+    per outer step, classical + modified Gram-Schmidt, Rayleigh-Ritz over the
+    active (unconverged) columns, restart when the workspace is full, convergence
+    of the first active Ritz pair at tol * max|theta|, lower filter bound moved
+    to the median active Ritz value.  After a convergence the next filter input is
+    the just-converged column, as the reference does (T1.py:596-597).
+    Returns (eigenvalues ascending, eigenvectors (n, k), iterations, converged)."""
+    assert spectrum_bound is not None, "ABORTED. The spectrum bound has to be initiated."
+    assert workspace_factor > 1, "ABORTED. We require User_WorkspaceSizeFactor > 1 "
+    rng = np.random.default_rng(seed)
+    jmin = min(n, k)
+    jmax = workspace_factor * jmin
+    V = np.zeros((n, jmax))
+    AV = np.zeros((n, jmax))
+    G = np.zeros((jmax, jmax))
+    conv = np.zeros(jmin + 1)
+    thb = spectrum_bound[-1] + 1e-5
+    x = rng.random(n)
+    x /= np.linalg.norm(x)
+    V[:, 0] = x
+    AV[:, 0] = op(x)
+    G[0, 0] = x @ AV[:, 0]
+    squeeze = (thb + G[0, 0]) / 2.0
+    beta = max(1e-14, abs(G[0, 0]))
+    tolr = tol * beta
+    nc, nc1, j = 0, 1, 1
+    for it in range(maxiter):
+        v = cdm_filter(op, x, degree, squeeze, thb)
+        v /= np.linalg.norm(v)
+        for _ in range(2):                           # ICGS against the whole basis
+            v -= V[:, :j] @ (V[:, :j].T @ v)
+        v /= np.linalg.norm(v)
+        for i in range(nc):                          # MGS against converged columns
+            v -= (V[:, i] @ v) * V[:, i]
+        V[:, j] = v
+        AV[:, j] = op(v)
+        r = V[:, nc:j + 1].T @ AV[:, j]
+        G[j, nc:j] = r[:-1]
+        G[nc:j + 1, j] = r
+        G = 0.5 * (G + G.T)
+        S, W = np.linalg.eigh(G[nc:j + 1, nc:j + 1])
+        if j + 1 >= jmax:
+            jr = max(nc1, jmin + 5, min(jmin + nc, jmax - 5))
+        else:
+            jr = j + 1
+        nn = jr - nc
+        V[:, nc:jr] = V[:, nc:j + 1] @ W[:, :nn]
+        AV[:, nc:jr] = AV[:, nc:j + 1] @ W[:, :nn]
+        G[nc:jr, nc:jr] = np.diag(S[:nn])
+        beta = max(beta, np.max(np.abs(S)))
+        tolr = tol * beta
+        theta = S[0]
+        x = V[:, nc].copy()
+        res = np.linalg.norm(AV[:, nc] - theta * x)
+        if res < tolr:
+            conv[nc] = theta
+            nc += 1
+            nc1 = nc + 1
+            if nc >= jmin:
+                lam = conv[:-1]
+                idx = np.argsort(lam)
+                return lam[idx], V[:, idx], it + 1, True
+            x = V[:, nc - 1].copy()
+        j = jr
+        squeeze = max(float(np.median(S)), spectrum_bound[0])
+    lam = conv[:-1]
+    idx = np.argsort(lam)
+    return lam[idx], V[:, idx], maxiter, False

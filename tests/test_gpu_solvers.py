@@ -223,3 +223,77 @@ def test_block_solvers_converge_in_tight_cluster_at_loose_tol(precision, lean):
     assert info["converged"] and info["iterations"] < 40
     assert info["max_rel_residual"] <= 1.5 * tol
     assert np.max(np.abs(S.cpu().numpy() - w[6:6 + k]) / w[6:6 + k]) < 1e-4
+
+
+def test_cdm_facade_matches_dense(small):
+    """Chebyshev-Davidson through the reference signature (no deflation: the six
+    rigid modes at PlusI come first), FP64 at tol 1e-10 -> eigenvalues to 1e-9."""
+    from inching_b200.Burn.ChebyshevDavidsonSubspaceIteration.T1 import (OOC2_KrylovAv_A_EstimateSpectrumBound,
+                                                                           S_HeigvalCDSIHD_HeigvecCDSIHD)
+    s = small
+    bound = OOC2_KrylovAv_A_EstimateSpectrumBound(None, s["H"])
+    S, V = S_HeigvalCDSIHD_HeigvecCDSIHD(s["H"], None, k=16, tol=1e-10, User_ChebyshevDegree=20,
+                                         User_SpectrumBound=bound)
+    ref = s["w"][:16]
+    assert np.max(np.abs(S.cpu().numpy() - ref) / ref) < 1e-9
+    Vh = V.cpu().numpy()
+    R = s["Hd"] @ Vh - Vh * S.cpu().numpy()[None, :]
+    assert np.linalg.norm(R, axis=0).max() < 1e-8 * np.abs(s["w"]).max()
+    assert max_cluster_angle(Vh, s["U"], s["w"], 0, 16) < 1e-5
+
+
+def test_cdm_facade_refusals(small):
+    from inching_b200.Burn.ChebyshevDavidsonSubspaceIteration.T1 import S_HeigvalCDSIHD_HeigvecCDSIHD
+    s = small
+    with pytest.raises(AssertionError, match="ABORTED"):
+        S_HeigvalCDSIHD_HeigvecCDSIHD(s["H"], None, k=4)
+    with pytest.raises(AssertionError, match="ABORTED"):
+        S_HeigvalCDSIHD_HeigvecCDSIHD(s["H"], None, k=4, User_SpectrumBound=(0.0, 60.0),
+                                      User_Q_HotellingDeflation=s["Q"])
+    with pytest.raises(AssertionError, match="ABORTED"):
+        S_HeigvalCDSIHD_HeigvecCDSIHD(s["H"], None, k=4, User_SpectrumBound=(0.0, 60.0), User_WorkspaceSizeFactor=1)
+
+
+@pytest.mark.parametrize("precision,block", [("f64", 1), ("mixed", 4)])
+def test_cdm_deflated_matches_dense(small, precision, block):
+    """Rigid modes projected out, single-vector FP64 and block-of-4 with the FP32
+    filter: the tolerance is on FP64 residuals in both, so eigenvalues to 1e-9."""
+    from inching_b200.solvers.cdm import cdm
+    from inching_b200.spectrum import estimate_spectrum_bound
+    s = small
+    bound = estimate_spectrum_bound(s["H"], steps=300)
+    S, V, info = cdm(s["H"], 24, tol=1e-10, Q=s["Q"], precision=precision, block=block, degree=20,
+                     spectrum_bound=bound, return_info=True)
+    assert info["converged"] and info["filter_graph_replays"] == info["iterations"]
+    ref = s["w"][6:30]
+    assert np.max(np.abs(S.cpu().numpy() - ref) / ref) < 1e-9
+    assert max_cluster_angle(V.cpu().numpy(), s["U"], s["w"], 6, 30) < 1e-5
+    assert np.abs(s["Q"].cpu().numpy() @ V.cpu().numpy()).max() < 1e-10
+
+
+def test_cdm_agrees_with_oracle_and_eager_filter(small):
+    """The GPU solver (graph-replayed filter and launch-by-launch filter) and the
+    oracle's restatement of the reference flow converge to the same eigenvalues."""
+    from inching_b200.solvers.cdm import cdm
+    s = small
+    Hs = oh.full_from_lower(s["A"], s["Ad"])
+    bound = (float(s["w"][0]), float(s["w"][-1]))
+    lo, _, its, ok = osv.cdm(lambda v: Hs @ v, Hs.shape[0], k=12, tol=1e-10, degree=20, spectrum_bound=bound)
+    assert ok
+    S1 = cdm(s["H"], 12, tol=1e-10, degree=20, spectrum_bound=bound)[0].cpu().numpy()
+    S2, _, i2 = cdm(s["H"], 12, tol=1e-10, degree=20, spectrum_bound=bound, cuda_graph=False, return_info=True)
+    assert i2["filter_graph_replays"] == 0
+    assert np.max(np.abs(S1 - lo) / lo) < 1e-9
+    assert np.max(np.abs(S2.cpu().numpy() - S1) / S1) < 1e-9
+
+
+def test_pipeline_cdm():
+    """normal_modes(..., solver="cdm"): the rigid modes projected out, results in
+    input atom order, same eigenvalues as the block solver."""
+    from inching_b200 import synth
+    from inching_b200.pipeline import normal_modes_device
+    Xd = torch.from_numpy(synth.globule(2000, seed=4) / 10.0).cuda()
+    e0, m0, _ = normal_modes_device(Xd, 12, tol=1e-9, precision="f64")
+    e1, m1, i1 = normal_modes_device(Xd, 12, solver="cdm", tol=1e-10, precision="mixed", block=4, degree=24)
+    assert i1["converged"]
+    assert float(((e1 - e0).abs() / e0).max()) < 1e-8
