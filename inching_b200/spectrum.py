@@ -23,8 +23,9 @@ from . import polyfilter
 from .krylov import HessianOperator
 
 
-def estimate_spectrum_bound(A, steps=300, seed=0, precision="f64"):
-    """(min, max) Ritz values of a `steps`-step Lanczos run from a random start."""
+def estimate_spectrum_bound(A, steps=300, seed=0, precision="f64", return_ritz=False):
+    """(min, max) Ritz values of a `steps`-step Lanczos run from a random start
+    (with return_ritz, also all Ritz values, ascending)."""
     dev = A.device
     N = A.shape[0]
     op = HessianOperator(A, prec=32 if precision == "mixed" else 64)
@@ -53,6 +54,8 @@ def estimate_spectrum_bound(A, steps=300, seed=0, precision="f64"):
     be = beta.cpu().numpy()
     T = np.diag(al) + np.diag(be, -1) + np.diag(be, 1)
     w = np.linalg.eigvalsh(T)
+    if return_ritz:
+        return float(w.min()), float(w.max()), w
     return float(w.min()), float(w.max())
 
 
