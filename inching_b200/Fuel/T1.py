@@ -19,8 +19,12 @@ class Xnumpy_SparseCupyMatrixUngappped:
     def __init__(self, X, batch_head=None, maxleafsize=100, rc_Gamma=8.0, device=None, User_PlusI=1.0,
                  dtype_temp=torch.float64, X_precision=None, NnzMinMaxDict=None, User_DictCharmmGuiPbc=None,
                  User_StorePrecisions=("f64", "f32")):
+        self.pbc = None
         if User_DictCharmmGuiPbc is not None:
-            raise NotImplementedError("periodic xy images (User_DictCharmmGuiPbc) are not supported by inching_b200")
+            from ..graph import pbc_box
+            self.pbc = pbc_box(User_DictCharmmGuiPbc)
+            assert self.pbc[0] > rc_Gamma / 10.0, "ABORTED. The PBC box size X is smaller than rc gamma."
+            assert self.pbc[1] > rc_Gamma / 10.0, "ABORTED. The PBC box size Y is smaller than rc gamma."
         if isinstance(device, int):
             device = torch.device("cuda", device)
         self.X = X
@@ -34,7 +38,7 @@ class Xnumpy_SparseCupyMatrixUngappped:
     def _build(self):
         if self._store is None:
             self._store = HessianStore(self.X, self.rc_Gamma * 10.0, plus_i=self.User_PlusI,
-                                       precisions=self.precisions, device=self.device)
+                                       precisions=self.precisions, device=self.device, pbc=self.pbc)
         return self._store
 
     def ReturnNumberTotalBatch(self):

@@ -56,6 +56,14 @@ _SIGS = {
                                             POINTER(c_int64), c_void_p, c_size_t, c_void_p]),
     "inch_neighbors_fill": (ctypes.c_int, [c_void_p, POINTER(CellGrid), c_double, c_void_p, c_void_p,
                                            c_void_p, c_size_t, c_void_p]),
+    "inch_neighbors_count_pbc_xy": (ctypes.c_int, [c_void_p, POINTER(CellGrid), c_double, c_double, c_double,
+                                                   c_void_p, c_void_p, POINTER(c_int64), c_void_p, c_size_t,
+                                                   c_void_p]),
+    "inch_neighbors_fill_pbc_xy": (ctypes.c_int, [c_void_p, POINTER(CellGrid), c_double, c_double, c_double,
+                                                  c_void_p, c_void_p, c_void_p, c_void_p, c_size_t, c_void_p]),
+    "inch_hessian_assemble_pbc_xy": (ctypes.c_int, [c_void_p, c_int64, c_double, c_double, c_void_p, c_void_p,
+                                                    c_void_p, c_double, c_double, c_void_p, c_void_p, c_void_p,
+                                                    c_void_p, c_void_p]),
     "inch_rcm_workspace_size": (c_size_t, [c_int64]),
     "inch_rcm": (ctypes.c_int, [c_void_p, c_void_p, c_void_p, c_void_p, c_int64, c_void_p, c_void_p,
                                 POINTER(c_int32), c_void_p, c_size_t, c_void_p]),
@@ -160,8 +168,10 @@ def _require_cuda(t, name, dtype=None):
 # ---------------------------------------------------------------------------
 # Neighbours, Cuthill-McKee, band slices
 # ---------------------------------------------------------------------------
-def neighbor_lists(X: torch.Tensor, rc_nm: float):
-    """(degree int32 (N,), rowptr int64 (N+1,), cols int32 (nnz,)) on X's device."""
+def neighbor_lists(X: torch.Tensor, rc_nm: float, box_xy=None):
+    """(degree int32 (N,), rowptr int64 (N+1,), cols int32 (nnz,)) on X's device;
+    with box_xy = (box_x, box_y) in nm, periodic xy images too, and a fourth
+    tensor: the image code (int8, nnz) of every entry."""
     _require_cuda(X, "X", torch.float64)
     L = lib()
     n = X.shape[0]
@@ -173,13 +183,23 @@ def neighbor_lists(X: torch.Tensor, rc_nm: float):
     degree = torch.empty(n, dtype=torch.int32, device=dev)
     rowptr = torch.empty(n + 1, dtype=torch.int64, device=dev)
     nnz = c_int64(0)
-    check(L.inch_neighbors_count(_ptr(X), ctypes.byref(grid), rc_nm, _ptr(degree), _ptr(rowptr),
-                                 ctypes.byref(nnz), _ptr(ws), ws.numel(), _stream()))
+    if box_xy is None:
+        check(L.inch_neighbors_count(_ptr(X), ctypes.byref(grid), rc_nm, _ptr(degree), _ptr(rowptr),
+                                     ctypes.byref(nnz), _ptr(ws), ws.numel(), _stream()))
+    else:
+        bx, by = float(box_xy[0]), float(box_xy[1])
+        check(L.inch_neighbors_count_pbc_xy(_ptr(X), ctypes.byref(grid), rc_nm, bx, by, _ptr(degree), _ptr(rowptr),
+                                            ctypes.byref(nnz), _ptr(ws), ws.numel(), _stream()))
     cols = torch.empty(max(nnz.value, 1), dtype=torch.int32, device=dev)[:nnz.value]
-    check(L.inch_neighbors_fill(_ptr(X), ctypes.byref(grid), rc_nm, _ptr(rowptr), _ptr(cols),
-                                _ptr(ws), ws.numel(), _stream()))
     _count(8)   # bbox, assign, scan, scatter, count, set0, scan, fill
-    return degree, rowptr, cols
+    if box_xy is None:
+        check(L.inch_neighbors_fill(_ptr(X), ctypes.byref(grid), rc_nm, _ptr(rowptr), _ptr(cols),
+                                    _ptr(ws), ws.numel(), _stream()))
+        return degree, rowptr, cols
+    image = torch.empty(max(nnz.value, 1), dtype=torch.int8, device=dev)[:nnz.value]
+    check(L.inch_neighbors_fill_pbc_xy(_ptr(X), ctypes.byref(grid), rc_nm, bx, by, _ptr(rowptr), _ptr(cols),
+                                       _ptr(image), _ptr(ws), ws.numel(), _stream()))
+    return degree, rowptr, cols, image
 
 
 def cuthill_mckee(rowptr, cols, degree, seed_order):
@@ -222,7 +242,8 @@ def band_slices(rowptr, cols, n_atoms, heads, gap=100, max_slices=256):
 # ---------------------------------------------------------------------------
 # Hessian store and operator
 # ---------------------------------------------------------------------------
-def hessian_assemble(X, rowptr, cols, rc_nm, plus_i, want64=True, want32=True, pair_weight=None):
+def hessian_assemble(X, rowptr, cols, rc_nm, plus_i, want64=True, want32=True, pair_weight=None, image=None,
+                     box_xy=None):
     _require_cuda(X, "X", torch.float64)
     _require_cuda(rowptr, "rowptr", torch.int64)
     _require_cuda(cols, "cols", torch.int32)
@@ -233,7 +254,13 @@ def hessian_assemble(X, rowptr, cols, rc_nm, plus_i, want64=True, want32=True, p
     diag64 = torch.empty((n, 8), dtype=torch.float64, device=dev) if want64 else None
     ent32 = torch.empty((nnz, 4), dtype=torch.float32, device=dev) if want32 else None
     diag32 = torch.empty((n, 8), dtype=torch.float32, device=dev) if want32 else None
-    if pair_weight is None:
+    if image is not None:
+        assert pair_weight is None, "ABORTED. periodic images and pair weights are not combined"
+        _require_cuda(image, "image", torch.int8)
+        check(lib().inch_hessian_assemble_pbc_xy(_ptr(X), n, rc_nm, plus_i, _ptr(rowptr), _ptr(cols), _ptr(image),
+                                                 float(box_xy[0]), float(box_xy[1]), _ptr(ent64), _ptr(diag64),
+                                                 _ptr(ent32), _ptr(diag32), _stream()))
+    elif pair_weight is None:
         check(lib().inch_hessian_assemble(_ptr(X), n, rc_nm, plus_i, _ptr(rowptr), _ptr(cols), _ptr(ent64),
                                           _ptr(diag64), _ptr(ent32), _ptr(diag32), _stream()))
     else:

@@ -43,12 +43,32 @@ struct GridDev {
 
 __device__ __forceinline__ int clampi(int v, int lo, int hi) { return v < lo ? lo : (v > hi ? hi : v); }
 
+// Cell of a point, clamped to the grid (in double, before the integer cast, so
+// periodic-image queries far outside the grid stay defined).  A clamped cell's
+// 3x3x3 neighbourhood still contains every atom within rc of the point.
+__device__ __forceinline__ int cell_axis(double v, double o, double inv, int d) {
+  const double f = fmin(fmax(floor((v - o) * inv), 0.0), static_cast<double>(d - 1));
+  return clampi(static_cast<int>(f), 0, d - 1);
+}
+
 __device__ __forceinline__ void cell_of(const GridDev& g, double x, double y, double z, int& cx, int& cy,
                                         int& cz) {
-  cx = clampi(static_cast<int>(floor((x - g.ox) * g.inv_cell)), 0, g.dx - 1);
-  cy = clampi(static_cast<int>(floor((y - g.oy) * g.inv_cell)), 0, g.dy - 1);
-  cz = clampi(static_cast<int>(floor((z - g.oz) * g.inv_cell)), 0, g.dz - 1);
+  cx = cell_axis(x, g.ox, g.inv_cell, g.dx);
+  cy = cell_axis(y, g.oy, g.inv_cell, g.dy);
+  cz = cell_axis(z, g.oz, g.inv_cell, g.dz);
 }
+
+// Periodic images in x and y, in the reference's instruction order
+// (Fuel/Coordinate/T1.py:98-107): centre, +x, -x, +y, -y, +x+y, +x-y, -x+y, -x-y.
+__device__ __forceinline__ void image_shift(int k, double bx, double by, double& sx, double& sy) {
+  const int ix = (k == 1 || k == 5 || k == 6) ? 1 : ((k == 2 || k == 7 || k == 8) ? -1 : 0);
+  const int iy = (k == 3 || k == 5 || k == 7) ? 1 : ((k == 4 || k == 6 || k == 8) ? -1 : 0);
+  sx = ix == 0 ? 0.0 : (ix > 0 ? bx : -bx);
+  sy = iy == 0 ? 0.0 : (iy > 0 ? by : -by);
+}
+
+constexpr int kImageShift = 27;                       // sort key = image << 27 | column (PBC rows)
+constexpr int kColMask = (1 << kImageShift) - 1;
 
 // Squared distance in cKDTree's operation order, no contraction.
 __device__ __forceinline__ double sqdist(double ax, double ay, double az, double bx, double by, double bz) {
@@ -128,20 +148,28 @@ __device__ __forceinline__ bool zrun(const GridDev& g, const int* __restrict__ c
   return true;
 }
 
+// NIMG = 1: plain cutoff graph; NIMG = 9: the query point is also shifted by
+// each periodic xy image (x_i + s, rounded once, as numpy's xx + box * instr).
+template <int NIMG>
 __global__ void k_count(const double4* __restrict__ sorted, int64_t n, GridDev g,
-                        const int* __restrict__ cell_start, double r2, int* __restrict__ degree,
-                        int64_t* __restrict__ deg64) {
+                        const int* __restrict__ cell_start, double r2, double bx, double by,
+                        int* __restrict__ degree, int64_t* __restrict__ deg64) {
   for (int64_t t = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; t < n; t += (int64_t)gridDim.x * blockDim.x) {
     double4 a = sorted[t];
-    int cx, cy, cz;
-    cell_of(g, a.x, a.y, a.z, cx, cy, cz);
     int cnt = 0;
-    for (int r = 0; r < 9; ++r) {
-      int beg, end;
-      if (!zrun(g, cell_start, cx, cy, cz, r, beg, end)) continue;
-      for (int p = beg; p < end; ++p) {
-        double4 b = sorted[p];
-        cnt += sqdist(a.x, a.y, a.z, b.x, b.y, b.z) <= r2;
+    for (int k = 0; k < NIMG; ++k) {
+      double sx = 0.0, sy = 0.0;
+      if (NIMG > 1) image_shift(k, bx, by, sx, sy);
+      const double qx = NIMG > 1 ? __dadd_rn(a.x, sx) : a.x, qy = NIMG > 1 ? __dadd_rn(a.y, sy) : a.y;
+      int cx, cy, cz;
+      cell_of(g, qx, qy, a.z, cx, cy, cz);
+      for (int r = 0; r < 9; ++r) {
+        int beg, end;
+        if (!zrun(g, cell_start, cx, cy, cz, r, beg, end)) continue;
+        for (int p = beg; p < end; ++p) {
+          double4 b = sorted[p];
+          cnt += sqdist(qx, qy, a.z, b.x, b.y, b.z) <= r2;
+        }
       }
     }
     int64_t i = static_cast<int64_t>(a.w);
@@ -150,37 +178,45 @@ __global__ void k_count(const double4* __restrict__ sorted, int64_t n, GridDev g
   }
 }
 
+template <int NIMG>
 __global__ void __launch_bounds__(kFillWarps * 32)
 k_fill(const double4* __restrict__ sorted, int64_t n, GridDev g, const int* __restrict__ cell_start,
-       double r2, const int64_t* __restrict__ rowptr, int* __restrict__ cols, int* __restrict__ err) {
+       double r2, double bx, double by, const int64_t* __restrict__ rowptr, int* __restrict__ cols,
+       int8_t* __restrict__ image, int* __restrict__ err) {
   __shared__ int buf[kFillWarps][kCap];
   const int w = threadIdx.x >> 5, lane = threadIdx.x & 31;
   int* s = buf[w];
   for (int64_t t = (int64_t)blockIdx.x * kFillWarps + w; t < n; t += (int64_t)gridDim.x * kFillWarps) {
     double4 a = sorted[t];
-    int cx, cy, cz;
-    cell_of(g, a.x, a.y, a.z, cx, cy, cz);
     int cnt = 0;
     bool over = false;
-    for (int r = 0; r < 9; ++r) {
-      int beg, end;
-      if (!zrun(g, cell_start, cx, cy, cz, r, beg, end)) continue;
-      for (int p0 = beg; p0 < end; p0 += 32) {
-        int p = p0 + lane;
-        bool ok = false;
-        int j = 0;
-        if (p < end) {
-          double4 b = sorted[p];
-          ok = sqdist(a.x, a.y, a.z, b.x, b.y, b.z) <= r2;
-          j = static_cast<int>(b.w);
+    for (int k = 0; k < NIMG; ++k) {
+      double sx = 0.0, sy = 0.0;
+      if (NIMG > 1) image_shift(k, bx, by, sx, sy);
+      const double qx = NIMG > 1 ? __dadd_rn(a.x, sx) : a.x, qy = NIMG > 1 ? __dadd_rn(a.y, sy) : a.y;
+      int cx, cy, cz;
+      cell_of(g, qx, qy, a.z, cx, cy, cz);
+      for (int r = 0; r < 9; ++r) {
+        int beg, end;
+        if (!zrun(g, cell_start, cx, cy, cz, r, beg, end)) continue;
+        for (int p0 = beg; p0 < end; p0 += 32) {
+          int p = p0 + lane;
+          bool ok = false;
+          int j = 0;
+          if (p < end) {
+            double4 b = sorted[p];
+            ok = sqdist(qx, qy, a.z, b.x, b.y, b.z) <= r2;
+            j = static_cast<int>(b.w);
+            if (NIMG > 1) j |= k << kImageShift;   // rows list image 0 first, then 1, ... (each sorted)
+          }
+          unsigned m = __ballot_sync(0xffffffffu, ok);
+          int pos = cnt + __popc(m & ((1u << lane) - 1u));
+          if (ok) {
+            if (pos < kCap) s[pos] = j;
+            else over = true;
+          }
+          cnt += __popc(m);
         }
-        unsigned m = __ballot_sync(0xffffffffu, ok);
-        int pos = cnt + __popc(m & ((1u << lane) - 1u));
-        if (ok) {
-          if (pos < kCap) s[pos] = j;
-          else over = true;
-        }
-        cnt += __popc(m);
       }
     }
     over = __any_sync(0xffffffffu, over);
@@ -211,7 +247,14 @@ k_fill(const double4* __restrict__ sorted, int64_t n, GridDev g, const int* __re
         __syncwarp();
       }
     }
-    for (int q = lane; q < cnt; q += 32) cols[row + q] = s[q];
+    for (int q = lane; q < cnt; q += 32) {
+      if (NIMG > 1) {
+        cols[row + q] = s[q] & kColMask;
+        image[row + q] = static_cast<int8_t>(s[q] >> kImageShift);
+      } else {
+        cols[row + q] = s[q];
+      }
+    }
     __syncwarp();
   }
 }
@@ -328,16 +371,18 @@ extern "C" size_t inch_neighbors_workspace_size(const inch_cell_grid* g) {
   return s.bytes();
 }
 
-extern "C" inch_status inch_neighbors_count(const double* X, const inch_cell_grid* grid, double rc,
-                                            int32_t* degree, int64_t* rowptr, int64_t* nnz_host, void* ws,
-                                            size_t ws_bytes, cudaStream_t stream) {
-  INCH_REQUIRE(X && grid && degree && rowptr && nnz_host, INCH_INVALID_ARG, "inch_neighbors_count: NULL argument");
-  INCH_REQUIRE(rc > 0 && grid->cell >= rc, INCH_INVALID_ARG, "inch_neighbors_count: cell edge below rc");
+namespace {
+template <int NIMG>
+inch_status neighbors_count_impl(const char* who, const double* X, const inch_cell_grid* grid, double rc, double bx,
+                                 double by, int32_t* degree, int64_t* rowptr, int64_t* nnz_host, void* ws,
+                                 size_t ws_bytes, cudaStream_t stream) {
+  INCH_REQUIRE(X && grid && degree && rowptr && nnz_host, INCH_INVALID_ARG, "%s: NULL argument", who);
+  INCH_REQUIRE(rc > 0 && grid->cell >= rc, INCH_INVALID_ARG, "%s: cell edge below rc", who);
   const int64_t n = grid->n_atoms;
   Carver c(ws, ws_bytes);
   NbrWs w;
   carve_nbr(c, *grid, &w);
-  INCH_REQUIRE(c.ok, INCH_OOM, "inch_neighbors_count: workspace of %zu bytes, need %zu", ws_bytes,
+  INCH_REQUIRE(c.ok, INCH_OOM, "%s: workspace of %zu bytes, need %zu", who, ws_bytes,
                inch_neighbors_workspace_size(grid));
   GridDev g = to_dev(*grid);
   INCH_CUDA(cudaMemsetAsync(w.cell_cnt, 0, sizeof(int) * (grid->ncells + 1), stream));
@@ -349,7 +394,7 @@ extern "C" inch_status inch_neighbors_count(const double* X, const inch_cell_gri
   INCH_CUDA(cub::DeviceScan::ExclusiveSum(w.cub_tmp, cb, w.cell_cnt, w.cell_start, (int)(grid->ncells + 1), stream));
   k_scatter<<<blocks, 256, 0, stream>>>(X, n, w.cell_start, w.cell_id, w.slot, w.sorted);
   INCH_LAUNCH_CHECK();
-  k_count<<<blocks, 256, 0, stream>>>(w.sorted, n, g, w.cell_start, rc * rc, degree, w.deg64);
+  k_count<NIMG><<<blocks, 256, 0, stream>>>(w.sorted, n, g, w.cell_start, rc * rc, bx, by, degree, w.deg64);
   INCH_LAUNCH_CHECK();
   k_set0<<<1, 1, 0, stream>>>(rowptr);
   INCH_LAUNCH_CHECK();
@@ -360,26 +405,71 @@ extern "C" inch_status inch_neighbors_count(const double* X, const inch_cell_gri
   return INCH_OK;
 }
 
-extern "C" inch_status inch_neighbors_fill(const double* X, const inch_cell_grid* grid, double rc,
-                                           const int64_t* rowptr, int32_t* cols, void* ws, size_t ws_bytes,
-                                           cudaStream_t stream) {
-  INCH_REQUIRE(X && grid && rowptr && cols, INCH_INVALID_ARG, "inch_neighbors_fill: NULL argument");
+template <int NIMG>
+inch_status neighbors_fill_impl(const char* who, const double* X, const inch_cell_grid* grid, double rc, double bx,
+                                double by, const int64_t* rowptr, int32_t* cols, int8_t* image, void* ws,
+                                size_t ws_bytes, cudaStream_t stream) {
+  INCH_REQUIRE(X && grid && rowptr && cols && (NIMG == 1 || image), INCH_INVALID_ARG, "%s: NULL argument", who);
   const int64_t n = grid->n_atoms;
   Carver c(ws, ws_bytes);
   NbrWs w;
   carve_nbr(c, *grid, &w);
-  INCH_REQUIRE(c.ok, INCH_OOM, "inch_neighbors_fill: workspace too small");
+  INCH_REQUIRE(c.ok, INCH_OOM, "%s: workspace too small", who);
   GridDev g = to_dev(*grid);
   INCH_CUDA(cudaMemsetAsync(w.err, 0, sizeof(int) * 4, stream));
   int blocks = grid_for(n, kFillWarps, 148 * 8);
-  k_fill<<<blocks, kFillWarps * 32, 0, stream>>>(w.sorted, n, g, w.cell_start, rc * rc, rowptr, cols, w.err);
+  k_fill<NIMG><<<blocks, kFillWarps * 32, 0, stream>>>(w.sorted, n, g, w.cell_start, rc * rc, bx, by, rowptr, cols,
+                                                       image, w.err);
   INCH_LAUNCH_CHECK();
   int herr = 0;
   INCH_CUDA(cudaMemcpyAsync(&herr, w.err, sizeof(int), cudaMemcpyDeviceToHost, stream));
   INCH_CUDA(cudaStreamSynchronize(stream));
-  INCH_REQUIRE(herr != 1, INCH_LIMIT, "inch_neighbors_fill: an atom has more than %d neighbours within the cutoff",
-               kCap);
-  INCH_REQUIRE(herr == 0, INCH_INVALID_ARG,
-               "inch_neighbors_fill: neighbour counts differ from inch_neighbors_count (different X or rc?)");
+  INCH_REQUIRE(herr != 1, INCH_LIMIT, "%s: an atom has more than %d neighbours within the cutoff", who, kCap);
+  INCH_REQUIRE(herr == 0, INCH_INVALID_ARG, "%s: neighbour counts differ from the count pass (different X or rc?)",
+               who);
   return INCH_OK;
+}
+
+inch_status check_box(const char* who, const inch_cell_grid* grid, double rc, double bx, double by) {
+  INCH_REQUIRE(grid != nullptr, INCH_INVALID_ARG, "%s: grid is NULL", who);
+  INCH_REQUIRE(std::isfinite(bx) && std::isfinite(by), INCH_INVALID_ARG, "%s: box sizes must be finite", who);
+  INCH_REQUIRE(bx > rc, INCH_INVALID_ARG, "ABORTED. The PBC box size X is smaller than rc gamma.");
+  INCH_REQUIRE(by > rc, INCH_INVALID_ARG, "ABORTED. The PBC box size Y is smaller than rc gamma.");
+  INCH_REQUIRE(grid->n_atoms < (int64_t(1) << kImageShift), INCH_INVALID_ARG,
+               "%s: periodic neighbour lists take at most 2^27 atoms", who);
+  return INCH_OK;
+}
+}  // namespace
+
+extern "C" inch_status inch_neighbors_count(const double* X, const inch_cell_grid* grid, double rc,
+                                            int32_t* degree, int64_t* rowptr, int64_t* nnz_host, void* ws,
+                                            size_t ws_bytes, cudaStream_t stream) {
+  return neighbors_count_impl<1>("inch_neighbors_count", X, grid, rc, 0.0, 0.0, degree, rowptr, nnz_host, ws,
+                                 ws_bytes, stream);
+}
+
+extern "C" inch_status inch_neighbors_count_pbc_xy(const double* X, const inch_cell_grid* grid, double rc,
+                                                   double box_x, double box_y, int32_t* degree, int64_t* rowptr,
+                                                   int64_t* nnz_host, void* ws, size_t ws_bytes,
+                                                   cudaStream_t stream) {
+  inch_status st = check_box("inch_neighbors_count_pbc_xy", grid, rc, box_x, box_y);
+  if (st != INCH_OK) return st;
+  return neighbors_count_impl<9>("inch_neighbors_count_pbc_xy", X, grid, rc, box_x, box_y, degree, rowptr,
+                                 nnz_host, ws, ws_bytes, stream);
+}
+
+extern "C" inch_status inch_neighbors_fill(const double* X, const inch_cell_grid* grid, double rc,
+                                           const int64_t* rowptr, int32_t* cols, void* ws, size_t ws_bytes,
+                                           cudaStream_t stream) {
+  return neighbors_fill_impl<1>("inch_neighbors_fill", X, grid, rc, 0.0, 0.0, rowptr, cols, nullptr, ws, ws_bytes,
+                                stream);
+}
+
+extern "C" inch_status inch_neighbors_fill_pbc_xy(const double* X, const inch_cell_grid* grid, double rc,
+                                                  double box_x, double box_y, const int64_t* rowptr, int32_t* cols,
+                                                  int8_t* image, void* ws, size_t ws_bytes, cudaStream_t stream) {
+  inch_status st = check_box("inch_neighbors_fill_pbc_xy", grid, rc, box_x, box_y);
+  if (st != INCH_OK) return st;
+  return neighbors_fill_impl<9>("inch_neighbors_fill_pbc_xy", X, grid, rc, box_x, box_y, rowptr, cols, image, ws,
+                                ws_bytes, stream);
 }

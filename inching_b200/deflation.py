@@ -11,6 +11,16 @@ import numpy as np
 import torch
 
 
+def translation_basis(n_atoms: int, device="cuda") -> torch.Tensor:
+    """(3, 3N) unit translations: the null space of an ANM with periodic xy
+    images, where rotations are no longer zero modes (the many-mode notebook keeps
+    only the three translations under PBC)."""
+    Q = torch.zeros((3, n_atoms, 3), dtype=torch.float64, device=device)
+    for a in range(3):
+        Q[a, :, a] = 1.0 / np.sqrt(n_atoms)
+    return Q.reshape(3, 3 * n_atoms)
+
+
 def rigid_body_basis(X_nm, device=None) -> torch.Tensor:
     """(6, 3N) float64 orthonormal rows on the device of X (or `device`)."""
     if isinstance(X_nm, torch.Tensor):

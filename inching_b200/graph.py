@@ -37,11 +37,25 @@ def to_device_coords(X, device=None) -> torch.Tensor:
     return t
 
 
-def neighbor_lists(X, rc_gamma_A: float = 8.0, device=None):
+def pbc_box(pbc):
+    """(box_x, box_y) in nm from the reference's User_DictCharmmGuiPbc
+    (RectBox_Xsize / RectBox_Ysize, same unit as X) or a (box_x, box_y) pair;
+    None stays None."""
+    if pbc is None:
+        return None
+    if isinstance(pbc, dict):
+        return float(pbc["RectBox_Xsize"]), float(pbc["RectBox_Ysize"])
+    return float(pbc[0]), float(pbc[1])
+
+
+def neighbor_lists(X, rc_gamma_A: float = 8.0, device=None, pbc=None):
     """Sorted neighbour lists within rc_Gamma (Angstrom; coordinates in nm), self
-    included.  Returns device tensors (degree int32, rowptr int64, cols int32)."""
+    included.  Returns device tensors (degree int32, rowptr int64, cols int32);
+    with pbc (User_DictCharmmGuiPbc or (box_x, box_y)) the periodic xy images
+    too, each row listing image 0's neighbours then image 1's, ..., and a fourth
+    tensor with every entry's image code (int8)."""
     Xd = to_device_coords(X, device)
-    return _native.neighbor_lists(Xd, rc_gamma_A / 10.0)
+    return _native.neighbor_lists(Xd, rc_gamma_A / 10.0, box_xy=pbc_box(pbc))
 
 
 def seed_order(degree: torch.Tensor) -> np.ndarray:
@@ -49,10 +63,17 @@ def seed_order(degree: torch.Tensor) -> np.ndarray:
     return np.argsort(degree.cpu().numpy())
 
 
-def cuthill_mckee(X, rc_gamma_A: float = 8.0, device=None, return_graph=False):
+def cuthill_mckee(X, rc_gamma_A: float = 8.0, device=None, return_graph=False, pbc=None):
     """Reversed Cuthill-McKee order of the cutoff graph of X (nm) and its inverse,
-    both as device int64 tensors (plus degree/rowptr/cols when return_graph)."""
-    degree, rowptr, cols = neighbor_lists(X, rc_gamma_A, device)
+    both as device int64 tensors (plus degree/rowptr/cols when return_graph).
+
+    With pbc the graph includes the periodic xy images.  The order is then a
+    valid reversed Cuthill-McKee order of that graph but not the reference's:
+    under PBC the reference's BFS reads each parent's neighbours in k-d-tree
+    traversal order (single-point queries there ignore return_sorted,
+    Fuel/Coordinate/T1.py:130-146), which this level-synchronous BFS does not
+    reproduce; degrees and neighbour sets are the reference's exactly."""
+    degree, rowptr, cols = neighbor_lists(X, rc_gamma_A, device, pbc=pbc)[:3]
     seeds = torch.from_numpy(seed_order(degree).astype(np.int64)).to(degree.device)
     order, undo, levels = _native.cuthill_mckee(rowptr, cols, degree, seeds)
     if return_graph:
@@ -87,13 +108,14 @@ def batch_heads(n_atoms: int, maxleafsize: int = 100) -> np.ndarray:
 
 
 def band_slices(X, rc_gamma_A: float = 8.0, maxleafsize: int = 1000, gap: int = 100, device=None,
-                graph=None):
+                graph=None, pbc=None):
     """Ungapped column slices per row batch and HalfNnz, as
-    X_KdUngappedMinMaxNeighbor (Fuel/Coordinate/T1.py:331-481) returns them."""
+    X_KdUngappedMinMaxNeighbor (Fuel/Coordinate/T1.py:331-481) returns them
+    (with pbc, over the neighbour lists that include periodic xy images)."""
     if graph is None:
-        degree, rowptr, cols = neighbor_lists(X, rc_gamma_A, device)
+        degree, rowptr, cols = neighbor_lists(X, rc_gamma_A, device, pbc=pbc)[:3]
     else:
-        degree, rowptr, cols = graph
+        degree, rowptr, cols = graph[:3]
     n = degree.shape[0]
     heads = torch.from_numpy(batch_heads(n, maxleafsize)).to(rowptr.device)
     max_slices = 256

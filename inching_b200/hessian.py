@@ -50,19 +50,26 @@ class HessianStore:
     order the caller wants (normally reversed Cuthill-McKee)."""
 
     def __init__(self, X_nm, rc_gamma_A: float = 8.0, plus_i: float = 1.0, precisions=("f64", "f32"),
-                 device=None, graph_=None, tiles=False, pair_weight=None):
+                 device=None, graph_=None, tiles=False, pair_weight=None, pbc=None):
         self.X = graph.to_device_coords(X_nm, device)
         self.device = self.X.device
         self.n_atoms = int(self.X.shape[0])
         self.rc_nm = rc_gamma_A / 10.0
         self.plus_i = float(plus_i)
+        self.box_xy = graph.pbc_box(pbc)     # periodic xy images (nm) or None
         if graph_ is None:
-            graph_ = _native.neighbor_lists(self.X, self.rc_nm)
-        self.degree, self.rowptr, self.cols = graph_
+            graph_ = _native.neighbor_lists(self.X, self.rc_nm, box_xy=self.box_xy)
+        self.degree, self.rowptr, self.cols = graph_[:3]
+        self.image = graph_[3] if len(graph_) > 3 else None
+        if (self.box_xy is None) != (self.image is None):
+            raise AssertionError("ABORTED. periodic images need both the box and the image codes of the lists")
+        if self.box_xy is not None and tiles:
+            raise AssertionError("ABORTED. the row-tile layout does not take periodic images")
         want64 = "f64" in precisions
         want32 = "f32" in precisions
         self.ent64, self.diag64, self.ent32, self.diag32 = _native.hessian_assemble(
-            self.X, self.rowptr, self.cols, self.rc_nm, self.plus_i, want64, want32, pair_weight=pair_weight)
+            self.X, self.rowptr, self.cols, self.rc_nm, self.plus_i, want64, want32, pair_weight=pair_weight,
+            image=self.image, box_xy=self.box_xy)
         n = 3 * self.n_atoms
         self.shape = (n, n)
         self.ndim = 2

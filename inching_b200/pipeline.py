@@ -50,7 +50,7 @@ def _solve(H, k, solver, precision, tol, Q, shift, seed, **kw):
 
 def normal_modes_device(X_nm: torch.Tensor, k: int, *, rc_gamma_A=8.0, plus_i=1.0, solver="chfsi",
                         precision="mixed", tol=1e-6, deflate_rigid=True, hotelling_shift=10.0, seed=0,
-                        warm_start=None, **kw):
+                        warm_start=None, pbc=None, **kw):
     """Lowest k non-rigid modes of the structure X_nm (CUDA (N,3) float64, nm).
 
     warm_start="coarse" (block solver only): initial block from the lowest modes
@@ -61,13 +61,24 @@ def normal_modes_device(X_nm: torch.Tensor, k: int, *, rc_gamma_A=8.0, plus_i=1.
 
     tol: for "chfsi", the relative residual ||Hv - lambda v|| <= tol*||H||; for the
     reference solvers, their own absolute tolerance.  Returns (eigval (k,) with
-    PlusI removed, eigvec (k, N, 3) in input atom order, info dict), on the GPU."""
+    PlusI removed, eigvec (k, N, 3) in input atom order, info dict), on the GPU.
+
+    pbc: periodic xy images (the reference's User_DictCharmmGuiPbc or
+    (box_x, box_y) in nm); the deflated null space is then the three translations."""
     t0 = time.perf_counter()
-    order, undo, (degree, _, _, levels) = graph.cuthill_mckee(X_nm, rc_gamma_A, return_graph=True)
+    order, undo, (degree, _, _, levels) = graph.cuthill_mckee(X_nm, rc_gamma_A, return_graph=True, pbc=pbc)
     Xr = X_nm[order]
     precisions = ("f64", "f32") if precision == "mixed" else ("f64",)
-    H = HessianStore(Xr, rc_gamma_A, plus_i=plus_i, precisions=precisions)
-    Q = rigid_body_basis(Xr) if deflate_rigid else None
+    H = HessianStore(Xr, rc_gamma_A, plus_i=plus_i, precisions=precisions, pbc=pbc)
+    if not deflate_rigid:
+        Q = None
+    elif pbc is not None:
+        from .deflation import translation_basis
+        Q = translation_basis(Xr.shape[0], device=Xr.device)
+    else:
+        Q = rigid_body_basis(Xr)
+    if pbc is not None and warm_start is not None:
+        raise AssertionError("ABORTED. the bead-model warm starts do not take periodic images")
     winfo = None
     if warm_start == "coarse":
         if solver != "chfsi":

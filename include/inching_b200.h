@@ -93,6 +93,23 @@ inch_status inch_neighbors_fill(const double* X_dev, const inch_cell_grid* grid_
                                 const int64_t* rowptr_dev, int32_t* cols_dev,
                                 void* ws_dev, size_t ws_bytes, cudaStream_t stream);
 
+/* Periodic images in x and y (membrane systems): atom j is a neighbour of i
+ * through image s when |x_j - (x_i + s)| <= rc, s in the nine shifts
+ * {0, +-box_x, +-box_y, +-box_x +-box_y} in the order centre, +x, -x, +y, -y,
+ * +x+y, +x-y, -x+y, -x-y.  degree counts every (j, image) pair; each row lists
+ * image 0's neighbours (ascending j), then image 1's, ..., with image_dev[e] the
+ * image code 0..8 of entry e.  Requires box_x, box_y > rc (the reference's
+ * "ABORTED. The PBC box size X/Y is smaller than rc gamma.") and N < 2^27.
+ * Same grid and workspace as the non-periodic pair of calls.
+ * Replaces X_cKDTreePbcXy.query_ball_point (Fuel/Coordinate/T1.py:67-161) as used
+ * by X_KdCuthillMckeeOrder / X_KdUngappedMinMaxNeighbor with User_DictCharmmGuiPbc. */
+inch_status inch_neighbors_count_pbc_xy(const double* X_dev, const inch_cell_grid* grid_host, double rc,
+                                        double box_x, double box_y, int32_t* degree_dev, int64_t* rowptr_dev,
+                                        int64_t* nnz_host, void* ws_dev, size_t ws_bytes, cudaStream_t stream);
+inch_status inch_neighbors_fill_pbc_xy(const double* X_dev, const inch_cell_grid* grid_host, double rc,
+                                       double box_x, double box_y, const int64_t* rowptr_dev, int32_t* cols_dev,
+                                       int8_t* image_dev, void* ws_dev, size_t ws_bytes, cudaStream_t stream);
+
 /* ---------------------------------------------------------------------------
  * Cuthill-McKee ordering (level-synchronous, bit-exact with the sequential BFS
  * of Fuel/Coordinate/T1.py:254-323).  seed_order_dev is np.argsort(degree) as
@@ -150,6 +167,18 @@ inch_status inch_hessian_assemble_weighted(const double* X_dev, int64_t n_atoms,
                                            const int64_t* rowptr_dev, const int32_t* cols_dev,
                                            const double* pair_weight_dev, double* ent64_dev, double* diag64_dev,
                                            float* ent32_dev, float* diag32_dev, cudaStream_t stream);
+
+/* Hessian of a structure with periodic xy images, from the lists of
+ * inch_neighbors_*_pbc_xy: entry e (found with the query x_i + s) gets the block
+ * of d = (x_j - s) - x_i, the reference's (x_j + box * instr) - x_i with
+ * instr = -s (a pair seen through two images contributes two blocks); the
+ * diagonal sums them all.
+ * Replaces the image loop of Xnumpy_SparseCupyMatrixUngappped (Fuel/T1.py:317-396). */
+inch_status inch_hessian_assemble_pbc_xy(const double* X_dev, int64_t n_atoms, double rc, double plus_i,
+                                         const int64_t* rowptr_dev, const int32_t* cols_dev,
+                                         const int8_t* image_dev, double box_x, double box_y, double* ent64_dev,
+                                         double* diag64_dev, float* ent32_dev, float* diag32_dev,
+                                         cudaStream_t stream);
 
 /* ---------------------------------------------------------------------------
  * Message-passing network kernels of the learned warm start (no reference

@@ -58,6 +58,45 @@ def neighbor_lists(X_nm: np.ndarray, rc_gamma_A: float = 8.0, cell=None):
     return deg, rowptr, np.concatenate(lists)
 
 
+IMAGES_XY = ((0, 0), (1, 0), (-1, 0), (0, 1), (0, -1), (1, 1), (1, -1), (-1, 1), (-1, -1))
+
+
+def neighbor_lists_pbc_xy(X_nm: np.ndarray, rc_gamma_A: float, box_xy):
+    """Neighbour lists with periodic xy images, as X_cKDTreePbcXy.query_ball_point
+    (InchingLiteInteger/Fuel/Coordinate/T1.py:67-161) builds them for a
+    multi-point query: for each image shift s in the instruction order
+    (T1.py:98-107) the query point is x_i + s (one rounding, numpy's
+    xx + box * instr), the distance rule is cKDTree's, each image's list is sorted
+    and the nine lists are concatenated.  The box sizes must exceed rc (T1.py:94-95).
+    Returns (degree int32, rowptr int64, cols int32, image int8)."""
+    X = np.ascontiguousarray(X_nm, dtype=np.float64)
+    n = X.shape[0]
+    rc = rc_gamma_A / 10.0
+    bx, by = float(box_xy[0]), float(box_xy[1])
+    assert bx > rc, "ABORTED. The PBC box size X is smaller than rc gamma."
+    assert by > rc, "ABORTED. The PBC box size Y is smaller than rc gamma."
+    r2 = rc * rc
+    lists, imgs = [[] for _ in range(n)], [[] for _ in range(n)]
+    for k, (ix, iy) in enumerate(IMAGES_XY):
+        shift = np.array([bx * ix, by * iy, 0.0])
+        Q = X + shift
+        for a in range(0, n, 512):
+            q = Q[a:a + 512]
+            d = X[None, :, :] - q[:, None, :]
+            s = d[..., 0] * d[..., 0]
+            s = s + d[..., 1] * d[..., 1]
+            s = s + d[..., 2] * d[..., 2]
+            for r in range(q.shape[0]):
+                js = np.nonzero(s[r] <= r2)[0].astype(np.int32)
+                lists[a + r].append(js)
+                imgs[a + r].append(np.full(len(js), k, np.int8))
+    rows = [np.concatenate(v) for v in lists]
+    deg = np.array([len(v) for v in rows], dtype=np.int32)
+    rowptr = np.zeros(n + 1, dtype=np.int64)
+    rowptr[1:] = np.cumsum(deg)
+    return deg, rowptr, np.concatenate(rows), np.concatenate([np.concatenate(v) for v in imgs])
+
+
 def cuthill_mckee(rowptr, cols, degree, seed_order=None, reverse=True):
     """Sequential k-d-tree Cuthill-McKee, restating
     InchingLiteInteger/Fuel/Coordinate/T1.py:254-323 over an adjacency list.

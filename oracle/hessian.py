@@ -12,7 +12,7 @@ from . import graph
 
 
 def hessian_lower(X_nm: np.ndarray, rc_gamma_A: float = 8.0, plus_i: float = 1.0,
-                  rowptr=None, cols=None):
+                  rowptr=None, cols=None, image=None, box_xy=None):
     """Lower triangle (incl. diagonal) of H + PlusI*I as CSR, and its diagonal.
 
     Restates InchingLiteInteger/Fuel/T1.py:276-455 without the row batching
@@ -25,15 +25,29 @@ def hessian_lower(X_nm: np.ndarray, rc_gamma_A: float = 8.0, plus_i: float = 1.0
         scalars (T1.py:410-421);
       * only scalars on or below the global diagonal are kept (tril, T1.py:444-449)
         and exact zeros are not stored (dense->CSR conversion).
+    With periodic xy images (box_xy given; lists from graph.neighbor_lists_pbc_xy
+    unless passed with their image codes): the reference's assembly loops over the
+    nine instructions for every (i, j) and forms (X_j + box * instr) - X_i
+    (Fuel/T1.py:332-334); the neighbour entry found with the query x_i + s is the
+    instruction -s, so its pair vector is (X_j - s) - X_i.  Blocks of the same
+    (i, j) through different images add up.
     Returns (A_lower csr (3N,3N), A_diag (3N,)).
     """
     X = np.ascontiguousarray(X_nm, dtype=np.float64)
     n = X.shape[0]
     rc = rc_gamma_A / 10.0
     if rowptr is None:
-        _, rowptr, cols = graph.neighbor_lists(X, rc_gamma_A)
+        if box_xy is None:
+            _, rowptr, cols = graph.neighbor_lists(X, rc_gamma_A)
+        else:
+            _, rowptr, cols, image = graph.neighbor_lists_pbc_xy(X, rc_gamma_A, box_xy)
     rows = np.repeat(np.arange(n), np.diff(rowptr))
-    d = X[cols] - X[rows]
+    if image is None:
+        d = X[cols] - X[rows]
+    else:
+        inst = np.asarray(graph.IMAGES_XY, dtype=np.float64)[np.asarray(image, dtype=np.int64)]
+        shift = np.stack([-inst[:, 0] * box_xy[0], -inst[:, 1] * box_xy[1], np.zeros(len(inst))], axis=1)
+        d = (X[cols] + shift) - X[rows]
     d2 = d[:, 0] * d[:, 0] + d[:, 1] * d[:, 1] + d[:, 2] * d[:, 2]
     mask = (d2 > rc ** 2) | (d2 == 0)
     with np.errstate(divide="ignore"):
@@ -43,7 +57,7 @@ def hessian_lower(X_nm: np.ndarray, rc_gamma_A: float = 8.0, plus_i: float = 1.0
     diag = np.zeros((n, 3, 3))
     np.add.at(diag, rows, -blocks)
     diag[:, [0, 1, 2], [0, 1, 2]] += plus_i
-    off = rows != cols
+    off = rows != cols if image is None else (rows != cols) | (np.asarray(image) != 0)
     bi = np.concatenate([rows[off], np.arange(n)])
     bj = np.concatenate([cols[off], np.arange(n)])
     bv = np.concatenate([blocks[off], diag])

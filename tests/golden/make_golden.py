@@ -130,6 +130,20 @@ def main(ref_root):
                         slice_ends=e, halfnnz=np.float64(halfnnz), **meta)
     print("globule5k", X.shape[0])
 
+    # periodic xy images: the reference's own X_cKDTreePbcXy on a seeded slab whose
+    # atoms lie inside the box (so its boundary shortcut changes nothing)
+    rng = np.random.default_rng(17)
+    box = np.array([3.6, 3.2, 4.0])
+    Xs = rng.random((2500, 3)) * box
+    pbc = {"RectBox_Xsize": box[0], "RectBox_Ysize": box[1], "RectBox_Zsize": box[2],
+           "X": (0.0, box[0]), "Y": (0.0, box[1]), "Z": (0.0, box[2])}
+    tree = coord.X_cKDTreePbcXy(Xs, User_DictCharmmGuiPbc=pbc)
+    nl = _quiet(tree.query_ball_point, Xs, 0.8)
+    deg = np.array([len(v) for v in nl], dtype=np.int32)
+    cols = np.concatenate([np.asarray(v, dtype=np.int32) for v in nl])
+    np.savez_compressed(os.path.join(HERE, "pbc_slab.npz"), X=Xs, box=box, degree=deg, cols=cols, **meta)
+    print("pbc_slab", Xs.shape[0], "deg", deg.mean())
+
     # Chebyshev filter design (pure numpy in the reference)
     windows = [
         dict(User_WantedInterval=(1.0, 1.05), User_SpectrumBound=(1.0, 120.0)),      # extremal

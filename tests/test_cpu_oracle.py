@@ -139,3 +139,37 @@ def test_oracle_cdm_matches_dense():
     assert np.abs(lam - w[:10]).max() < 1e-9 * w[-1]
     R = H @ V - V * lam[None, :]
     assert np.linalg.norm(R, axis=0).max() < 1e-8 * w[-1]
+
+
+def test_oracle_pbc_xy_neighbours_match_reference_golden():
+    """Periodic xy neighbour lists: the oracle's restatement against the lists the
+    reference's X_cKDTreePbcXy produced (degree pass form: per image sorted,
+    images concatenated in instruction order)."""
+    g = np.load(os.path.join(GOLDEN, "pbc_slab.npz"))
+    deg, rowptr, cols, image = og.neighbor_lists_pbc_xy(g["X"], 8.0, g["box"][:2])
+    assert np.array_equal(deg, g["degree"])
+    assert np.array_equal(cols, g["cols"])
+    # some rows really use images, and within a row each image block is sorted
+    assert (image > 0).sum() > 0.1 * len(image)
+    for i in range(0, len(deg), 97):
+        seg_c, seg_i = cols[rowptr[i]:rowptr[i + 1]], image[rowptr[i]:rowptr[i + 1]]
+        assert np.all(np.diff(seg_i) >= 0)
+        for k in np.unique(seg_i):
+            assert np.all(np.diff(seg_c[seg_i == k]) > 0)
+
+
+def test_oracle_pbc_hessian_translation_invariant():
+    """With periodic images the three translations stay null vectors of the ANM
+    part (rotations do not): H t = PlusI t."""
+    g = np.load(os.path.join(GOLDEN, "pbc_slab.npz"))
+    X = g["X"][:600] * np.array([1.0, 1.0, 1.0])
+    A, Ad = oh.hessian_lower(X, 8.0, 1.0, box_xy=g["box"][:2])
+    H = oh.full_from_lower(A, Ad)
+    n = X.shape[0]
+    for a in range(3):
+        t = np.zeros((n, 3))
+        t[:, a] = 1.0
+        t = t.ravel()
+        assert np.abs(H @ t - t).max() < 1e-10
+    r = np.cross(X - X.mean(0), np.array([0.0, 0.0, 1.0])).ravel()
+    assert np.abs(H @ r - r).max() > 1e-3
