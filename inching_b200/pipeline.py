@@ -116,4 +116,11 @@ def normal_modes(X, k: int, *, units="nm", **kw):
     Xd = torch.from_numpy(np.ascontiguousarray(Xh)).pin_memory().to("cuda", non_blocking=True)
     evals, modes, info = normal_modes_device(Xd, k, **kw)
     ev = evals.cpu().numpy()
-    return ev, modes.cpu().numpy(), info
+    # The (k, N, 3) float64 modes are read back into page-locked memory from torch's
+    # caching host allocator: ~50 GB/s instead of ~2 GB/s into fresh pageable pages
+    # (614 MB for 256 modes of 100k atoms: 12 ms instead of 0.3 s).  The returned
+    # array keeps that block alive; it is reused only after the array is released.
+    out = torch.empty(modes.shape, dtype=modes.dtype, pin_memory=True)
+    out.copy_(modes, non_blocking=True)
+    torch.cuda.current_stream().synchronize()
+    return ev, out.numpy(), info
