@@ -75,6 +75,8 @@ def batched_normal_modes(structs, k=32, *, units="nm", rc_gamma_A=8.0, plus_i=1.
                          degree=24, bucket_ratio=1.6, seed=0, verbose=False, profile=False, warm_start=None):
     t0 = time.perf_counter()
     structs = [np.asarray(X, dtype=np.float64) / (10.0 if units == "A" else 1.0) for X in structs]
+    if not structs:
+        return [], dict(buckets=[], seconds=0.0, structures=0)
     sizes = np.array([X.shape[0] for X in structs])
     results = [None] * len(structs)
     infos = []
@@ -118,3 +120,57 @@ def batched_normal_modes(structs, k=32, *, units="nm", rc_gamma_A=8.0, plus_i=1.
         infos.append(info)
     torch.cuda.synchronize()
     return results, dict(buckets=infos, seconds=time.perf_counter() - t0, structures=len(structs))
+
+
+# ---------------------------------------------------------------------------
+# Several GPUs: the structures are independent, so the batch shards with no
+# data-path collective (one process per GPU, torch.distributed for the plumbing).
+# ---------------------------------------------------------------------------
+def partition_by_size(sizes, world_size):
+    """Greedy size-balanced partition: structures in decreasing size, each to the
+    rank with the fewest atoms so far.  Returns one ascending index list per rank."""
+    sizes = np.asarray(sizes)
+    load = np.zeros(world_size, dtype=np.int64)
+    parts = [[] for _ in range(world_size)]
+    for i in np.argsort(-sizes, kind="stable"):
+        r = int(np.argmin(load))
+        parts[r].append(int(i))
+        load[r] += int(sizes[i])
+    return [sorted(p) for p in parts]
+
+
+def gather_results(local, dst=0):
+    """Collect every rank's {structure index: (eigenvalues, modes)} (host arrays) on
+    rank dst; the final and only exchange of the sharded batch.  Other ranks get None."""
+    import torch.distributed as dist
+    from .replicas import world
+    W, R = world()
+    if W == 1:
+        return dict(local)
+    out = [None] * W if R == dst else None
+    dist.gather_object(list(local.items()), out, dst=dst)
+    if R != dst:
+        return None
+    merged = {}
+    for part in out:
+        merged.update(dict(part))
+    return merged
+
+
+def sharded_batched_normal_modes(structs, k=32, *, gather=True, **kw):
+    """batched_normal_modes over this rank's share of `structs` (partition_by_size
+    over the ranks of the default process group; a single process takes all).
+    Returns ({index: (eigenvalues, modes)} -- every structure's, as host arrays, on
+    rank 0 after the gather; this rank's, modes on the device, without it -- and
+    this rank's info with its indices)."""
+    from .replicas import world
+    W, R = world()
+    sizes = [np.asarray(X).shape[0] for X in structs]
+    mine = partition_by_size(sizes, W)[R]
+    res, info = batched_normal_modes([structs[i] for i in mine], k, **kw)
+    info = dict(info, indices=mine, rank=R, world=W, atoms=int(sum(sizes[i] for i in mine)))
+    local = {i: r for i, r in zip(mine, res)}
+    if not gather:
+        return local, info
+    host = {i: (ev, m.cpu().numpy()) for i, (ev, m) in local.items()}
+    return gather_results(host), info

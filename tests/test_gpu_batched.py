@@ -57,3 +57,18 @@ def test_segmented_epilogue_matches_oracle(prec):
     H.matmul_seg(Xt, Yt, torch.from_numpy(seg).cuda(), torch.from_numpy(coef).cuda(), Yin=Yt, prec=prec)
     tol = (1e-12 if prec == 64 else 2e-6) * np.abs(ref).max() * 50
     assert np.abs(Yt.double().cpu().numpy() - ref).max() <= tol
+
+
+def test_sharded_batch_in_one_process_equals_batched():
+    """With one process the sharded entry point takes every structure and its
+    gathered host results equal the batched solve's."""
+    from inching_b200 import synth
+    from inching_b200.batched import batched_normal_modes, sharded_batched_normal_modes
+    structs = [synth.globule(n, seed=70 + i) / 10.0 for i, n in enumerate([400, 900, 650, 1500])]
+    res, _ = batched_normal_modes(structs, k=8, tol=1e-8, precision="f64")
+    merged, info = sharded_batched_normal_modes(structs, k=8, tol=1e-8, precision="f64")
+    assert info["indices"] == [0, 1, 2, 3] and sorted(merged) == [0, 1, 2, 3]
+    for i, (ev, modes) in enumerate(res):
+        ev2, m2 = merged[i]
+        assert np.max(np.abs(ev2 - ev) / ev) < 1e-9
+        assert m2.shape == tuple(modes.shape)
