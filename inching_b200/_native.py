@@ -61,6 +61,23 @@ _SIGS = {
                                                    c_void_p]),
     "inch_neighbors_fill_pbc_xy": (ctypes.c_int, [c_void_p, POINTER(CellGrid), c_double, c_double, c_double,
                                                   c_void_p, c_void_p, c_void_p, c_void_p, c_size_t, c_void_p]),
+    "inch_cheb_filter": (ctypes.c_int, [c_int32, c_int64, c_void_p, c_void_p, c_void_p, c_void_p, c_int64, c_int32,
+                                        c_int32, POINTER(c_double), c_double, c_double, c_void_p, c_int64, c_void_p,
+                                        c_void_p, c_int64, c_void_p]),
+    "inch_cheb_filter_scaled": (ctypes.c_int, [c_int32, c_int64, c_void_p, c_void_p, c_void_p, c_void_p, c_int64,
+                                               c_int32, c_int32, c_double, c_double, c_double, c_void_p, c_int64,
+                                               c_void_p, c_int64, c_void_p]),
+    "inch_block_orth_workspace_size": (c_size_t, [c_int32, c_int64]),
+    "inch_block_orth": (ctypes.c_int, [c_int64, c_int32, c_void_p, c_int64, c_void_p, c_int64, c_int64, c_void_p,
+                                       c_int64, c_int64, c_int32, c_void_p, c_size_t, c_void_p]),
+    "inch_rr_workspace_size": (c_size_t, []),
+    "inch_rr_project": (ctypes.c_int, [c_int64, c_int32, c_void_p, c_int64, c_void_p, c_int64, c_void_p, c_void_p,
+                                       c_size_t, c_void_p]),
+    "inch_rr_rotate": (ctypes.c_int, [c_int64, c_int32, c_int32, c_void_p, c_int64, c_void_p, c_void_p, c_int64,
+                                      c_void_p, c_size_t, c_void_p]),
+    "inch_residual_workspace_size": (c_size_t, [c_int32]),
+    "inch_residual_fp64": (ctypes.c_int, [c_int64, c_int32, c_void_p, c_int64, c_void_p, c_int64, c_void_p, c_void_p,
+                                          c_void_p, c_size_t, c_void_p]),
     "inch_hessian_assemble_pbc_xy": (ctypes.c_int, [c_void_p, c_int64, c_double, c_double, c_void_p, c_void_p,
                                                     c_void_p, c_double, c_double, c_void_p, c_void_p, c_void_p,
                                                     c_void_p, c_void_p]),
@@ -396,3 +413,78 @@ def mp(name, *args):
     conv = [(_ptr(a) if isinstance(a, torch.Tensor) else a) for a in args]
     check(getattr(lib(), "inch_mp_" + name)(*conv, _stream()))
     _count(1)
+
+
+# ---------------------------------------------------------------------------
+# Solver building blocks (C-ABI forms; the Python solvers use torch for the same
+# dense steps, these serve non-Python hosts and are checked against them)
+# ---------------------------------------------------------------------------
+def _ld(t):
+    return 1 if t.dim() == 1 else t.stride(0)
+
+
+def cheb_filter(prec, n_atoms, rowptr, ent, diag, X, mu, cc, dd):
+    """Y = sum_k mu[k] T_k((H - cc)/dd) X through inch_cheb_filter."""
+    b = X.shape[1]
+    Y = torch.empty_like(X)
+    W1 = torch.empty_like(X)
+    W2 = torch.empty_like(X)
+    mu_h = (c_double * len(mu))(*[float(m) for m in mu])
+    check(lib().inch_cheb_filter(prec, n_atoms, _ptr(rowptr), _ptr(ent), _ptr(diag), _ptr(X), _ld(X), b,
+                                 len(mu) - 1, mu_h, cc, dd, _ptr(Y), _ld(Y), _ptr(W1), _ptr(W2), _ld(W1), _stream()))
+    _count(len(mu) + 1)
+    return Y
+
+
+def cheb_filter_scaled(prec, n_atoms, rowptr, ent, diag, X, degree, a, b_up, a0):
+    b = X.shape[1]
+    Y = torch.empty_like(X)
+    W = torch.empty_like(X)
+    check(lib().inch_cheb_filter_scaled(prec, n_atoms, _ptr(rowptr), _ptr(ent), _ptr(diag), _ptr(X), _ld(X), b,
+                                        degree, a, b_up, a0, _ptr(Y), _ld(Y), _ptr(W), _ld(W), _stream()))
+    _count(degree + 1)
+    return Y
+
+
+def block_orth(Y, B1=None, B2=None, passes=2):
+    """In place: Y <- orthonormal basis of (I - B B^T) Y (FP64, row bases B1, B2)."""
+    _require_cuda(Y, "Y", torch.float64)
+    n, b = Y.shape
+    r1 = 0 if B1 is None else B1.shape[0]
+    r2 = 0 if B2 is None else B2.shape[0]
+    L = lib()
+    ws = _ws(L.inch_block_orth_workspace_size(b, max(r1, r2)), Y.device)
+    check(L.inch_block_orth(n, b, _ptr(Y), _ld(Y), _ptr(B1), r1, 0 if B1 is None else B1.stride(0), _ptr(B2), r2,
+                            0 if B2 is None else B2.stride(0), passes, _ptr(ws), ws.numel(), _stream()))
+    return Y
+
+
+def rr_project(Y, HY):
+    n, b = Y.shape
+    G = torch.empty((b, b), dtype=torch.float64, device=Y.device)
+    L = lib()
+    ws = _ws(L.inch_rr_workspace_size(), Y.device)
+    check(L.inch_rr_project(n, b, _ptr(Y), _ld(Y), _ptr(HY), _ld(HY), _ptr(G), _ptr(ws), ws.numel(), _stream()))
+    return G          # column-major storage of a symmetric matrix: same values either way
+
+
+def rr_rotate(Y, W, m):
+    """Z = Y W[:, :m] for W with eigenvectors in columns (torch/numpy convention)."""
+    n, b = Y.shape
+    Wc = W.t().contiguous()          # column-major W
+    Z = torch.empty((n, m), dtype=torch.float64, device=Y.device)
+    L = lib()
+    ws = _ws(L.inch_rr_workspace_size(), Y.device)
+    check(L.inch_rr_rotate(n, b, m, _ptr(Y), _ld(Y), _ptr(Wc), _ptr(Z), _ld(Z), _ptr(ws), ws.numel(), _stream()))
+    return Z
+
+
+def residual_fp64(HY, Y, theta):
+    n, b = Y.shape
+    res = torch.empty(b, dtype=torch.float64, device=Y.device)
+    L = lib()
+    ws = _ws(L.inch_residual_workspace_size(b), Y.device)
+    check(L.inch_residual_fp64(n, b, _ptr(HY), _ld(HY), _ptr(Y), _ld(Y), _ptr(theta.contiguous()), _ptr(res),
+                               _ptr(ws), ws.numel(), _stream()))
+    _count(2)
+    return res

@@ -64,7 +64,10 @@ def build(force: bool = False, verbose: bool = False) -> str:
         msg = "\n".join(f"--- {s}\n{o}" for s, o in failed)
         raise RuntimeError(f"nvcc failed:\n{msg}")
     tmp = LIB + ".tmp"
-    cmd = [NVCC, "-shared", "-gencode", "arch=compute_100a,code=sm_100a", *objs, "-o", tmp]
+    # cuBLAS for the tall-skinny GEMMs of the block-solver entry points; the rpath
+    # finds the toolkit's copy when no other libcublas.so.12 is loaded already
+    cmd = [NVCC, "-shared", "-gencode", "arch=compute_100a,code=sm_100a", *objs, "-lcublas",
+           "-Xlinker", "-rpath=/usr/local/cuda/lib64", "-o", tmp]
     r = subprocess.run(cmd, stdout=subprocess.PIPE, stderr=subprocess.STDOUT)
     if r.returncode != 0:
         raise RuntimeError("link failed:\n" + r.stdout.decode())

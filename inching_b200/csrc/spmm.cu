@@ -665,3 +665,133 @@ extern "C" inch_status inch_spmm_seg(int32_t prec, int64_t n_atoms, const int64_
   INCH_REQUIRE(err == cudaSuccess, INCH_CUDA_ERROR, "inch_spmm_seg: %s", cudaGetErrorString(err));
   return INCH_OK;
 }
+
+// ---------------------------------------------------------------------------
+// Chebyshev filters as single library calls (the SpMM above, looped inside the
+// library with its fused epilogue; the caller provides every buffer).
+// ---------------------------------------------------------------------------
+namespace inch {
+namespace {
+
+// Y = s * X over an (n, b) block with leading dimensions.
+template <class T>
+__global__ void k_scale_copy(const T* __restrict__ X, int64_t ldx, T* __restrict__ Y, int64_t ldy, int64_t n, int b,
+                             double s) {
+  for (int64_t t = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; t < n * b; t += (int64_t)gridDim.x * blockDim.x) {
+    const int64_t i = t / b;
+    const int c = static_cast<int>(t % b);
+    Y[i * ldy + c] = static_cast<T>(s * static_cast<double>(X[i * ldx + c]));
+  }
+}
+
+template <class T>
+inch_status cheb_mu(int64_t n_atoms, const int64_t* rowptr, const void* ent, const void* diag, const T* X,
+                    int64_t ldx, int b, int degree, const double* mu, double cc, double dd, T* Y, int64_t ldy, T* W1,
+                    T* W2, int64_t ldw, cudaStream_t s) {
+  const int64_t n = 3 * n_atoms;
+  k_scale_copy<T><<<grid_for(n * b, 256, 148 * 16), 256, 0, s>>>(X, ldx, Y, ldy, n, b, mu[0]);
+  INCH_LAUNCH_CHECK();
+  if (degree == 0) return INCH_OK;
+  // X_1 = (H X_0 - cc X_0) / dd;  Y += mu_1 X_1
+  Epi ep{1.0 / dd, -cc / dd, 0.0, mu[1], 0, 1, 0};
+  cudaError_t e = run<T>(n_atoms, rowptr, ent, diag, X, ldx, b, W1, ldw, nullptr, 0, Y, ldy, ep, nullptr, 0.0,
+                         nullptr, nullptr, s);
+  INCH_REQUIRE(e == cudaSuccess, INCH_CUDA_ERROR, "inch_cheb_filter: %s", cudaGetErrorString(e));
+  // X_{k+1} = 2 (H X_k - cc X_k) / dd - X_{k-1};  Y += mu_{k+1} X_{k+1}.  X_2 goes
+  // to W2; from then on X_{k+1} is written over X_{k-1} (never over the input X).
+  const T* prev = X;
+  int64_t ldprev = ldx;
+  T* cur = W1;
+  for (int k = 1; k < degree; ++k) {
+    T* out = (k == 1) ? W2 : const_cast<T*>(prev);
+    Epi ek{2.0 / dd, -2.0 * cc / dd, -1.0, mu[k + 1], 0, 1, 1};
+    e = run<T>(n_atoms, rowptr, ent, diag, cur, ldw, b, out, ldw, prev, ldprev, Y, ldy, ek, nullptr, 0.0, nullptr,
+               nullptr, s);
+    INCH_REQUIRE(e == cudaSuccess, INCH_CUDA_ERROR, "inch_cheb_filter: %s", cudaGetErrorString(e));
+    prev = cur;
+    ldprev = ldw;
+    cur = out;
+  }
+  return INCH_OK;
+}
+
+template <class T>
+inch_status cheb_scaled(int64_t n_atoms, const int64_t* rowptr, const void* ent, const void* diag, const T* X,
+                        int64_t ldx, int b, int degree, double a, double bup, double a0, T* Y, int64_t ldy, T* W,
+                        int64_t ldw, cudaStream_t s) {
+  // Zhou & Saad's scaled filter: Y_1 = (sigma_1 / e)(H X - c X), then
+  // Y_{t+1} = (2 sigma_{t+1} / e)(H Y_t - c Y_t) - sigma_t sigma_{t+1} Y_{t-1}.
+  const double e = (bup - a) / 2.0, c = (bup + a) / 2.0;
+  double sigma = e / (a0 - c);
+  const double sigma1 = sigma, tau = 2.0 / sigma1;
+  Epi ep{sigma1 / e, -sigma1 * c / e, 0.0, 0.0, 0, 0, 0};
+  cudaError_t err = run<T>(n_atoms, rowptr, ent, diag, X, ldx, b, Y, ldy, nullptr, 0, nullptr, 0, ep, nullptr, 0.0,
+                           nullptr, nullptr, s);
+  INCH_REQUIRE(err == cudaSuccess, INCH_CUDA_ERROR, "inch_cheb_filter_scaled: %s", cudaGetErrorString(err));
+  // buffers: older -> newer; the newest of the two sits in `cur`
+  const T* older = X;
+  int64_t ldo = ldx;
+  T* cur = Y;
+  int64_t ldc = ldy;
+  for (int t = 2; t <= degree; ++t) {
+    const double s2 = 1.0 / (tau - sigma);
+    T* out = (t == 2) ? W : const_cast<T*>(older);       // overwrite the oldest (never X)
+    const int64_t ldout = (t == 2) ? ldw : ldo;
+    Epi et{2.0 * s2 / e, -2.0 * s2 * c / e, -sigma * s2, 0.0, 0, 0, 1};
+    err = run<T>(n_atoms, rowptr, ent, diag, cur, ldc, b, out, ldout, older, ldo, nullptr, 0, et, nullptr, 0.0,
+                 nullptr, nullptr, s);
+    INCH_REQUIRE(err == cudaSuccess, INCH_CUDA_ERROR, "inch_cheb_filter_scaled: %s", cudaGetErrorString(err));
+    older = cur;
+    ldo = ldc;
+    cur = out;
+    ldc = ldout;
+    sigma = s2;
+  }
+  if (cur != Y) {
+    INCH_CUDA(cudaMemcpy2DAsync(Y, ldy * sizeof(T), cur, ldc * sizeof(T), b * sizeof(T), 3 * n_atoms,
+                                cudaMemcpyDeviceToDevice, s));
+  }
+  return INCH_OK;
+}
+
+}  // namespace
+}  // namespace inch
+
+extern "C" inch_status inch_cheb_filter(int32_t prec, int64_t n_atoms, const int64_t* rowptr, const void* ent,
+                                        const void* diag, const void* X, int64_t ldx, int32_t b, int32_t degree,
+                                        const double* mu_host, double cc, double dd, void* Y, int64_t ldy, void* W1,
+                                        void* W2, int64_t ldw, cudaStream_t stream) {
+  INCH_REQUIRE(prec == 32 || prec == 64, INCH_INVALID_ARG, "inch_cheb_filter: prec must be 32 or 64");
+  INCH_REQUIRE(rowptr && ent && diag && X && Y && mu_host && (degree == 0 || (W1 && W2)), INCH_INVALID_ARG,
+               "inch_cheb_filter: NULL argument");
+  INCH_REQUIRE(n_atoms >= 1 && b >= 1 && degree >= 0, INCH_INVALID_ARG, "inch_cheb_filter: bad sizes");
+  INCH_REQUIRE(dd != 0.0 && std::isfinite(cc) && std::isfinite(dd), INCH_INVALID_ARG,
+               "inch_cheb_filter: dd must be finite and non-zero");
+  INCH_REQUIRE(ldx >= b && ldy >= b && (degree == 0 || ldw >= b), INCH_INVALID_ARG,
+               "inch_cheb_filter: leading dimension below b");
+  INCH_REQUIRE(X != Y && X != W1 && X != W2 && Y != W1 && Y != W2 && (degree == 0 || W1 != W2), INCH_INVALID_ARG,
+               "inch_cheb_filter: X, Y, W1 and W2 must be distinct");
+  if (prec == 32)
+    return cheb_mu<float>(n_atoms, rowptr, ent, diag, static_cast<const float*>(X), ldx, b, degree, mu_host, cc, dd,
+                          static_cast<float*>(Y), ldy, static_cast<float*>(W1), static_cast<float*>(W2), ldw, stream);
+  return cheb_mu<double>(n_atoms, rowptr, ent, diag, static_cast<const double*>(X), ldx, b, degree, mu_host, cc, dd,
+                         static_cast<double*>(Y), ldy, static_cast<double*>(W1), static_cast<double*>(W2), ldw, stream);
+}
+
+extern "C" inch_status inch_cheb_filter_scaled(int32_t prec, int64_t n_atoms, const int64_t* rowptr,
+                                               const void* ent, const void* diag, const void* X, int64_t ldx,
+                                               int32_t b, int32_t degree, double a, double b_up, double a0, void* Y,
+                                               int64_t ldy, void* W, int64_t ldw, cudaStream_t stream) {
+  INCH_REQUIRE(prec == 32 || prec == 64, INCH_INVALID_ARG, "inch_cheb_filter_scaled: prec must be 32 or 64");
+  INCH_REQUIRE(rowptr && ent && diag && X && Y && W, INCH_INVALID_ARG, "inch_cheb_filter_scaled: NULL argument");
+  INCH_REQUIRE(n_atoms >= 1 && b >= 1 && degree >= 1, INCH_INVALID_ARG, "inch_cheb_filter_scaled: bad sizes");
+  INCH_REQUIRE(a0 < a && a < b_up && std::isfinite(a0) && std::isfinite(b_up), INCH_INVALID_ARG,
+               "inch_cheb_filter_scaled: need a0 < a < b_up");
+  INCH_REQUIRE(ldx >= b && ldy >= b && ldw >= b, INCH_INVALID_ARG, "inch_cheb_filter_scaled: leading dimension below b");
+  INCH_REQUIRE(X != Y && X != W && Y != W, INCH_INVALID_ARG, "inch_cheb_filter_scaled: X, Y and W must be distinct");
+  if (prec == 32)
+    return cheb_scaled<float>(n_atoms, rowptr, ent, diag, static_cast<const float*>(X), ldx, b, degree, a, b_up, a0,
+                              static_cast<float*>(Y), ldy, static_cast<float*>(W), ldw, stream);
+  return cheb_scaled<double>(n_atoms, rowptr, ent, diag, static_cast<const double*>(X), ldx, b, degree, a, b_up, a0,
+                             static_cast<double*>(Y), ldy, static_cast<double*>(W), ldw, stream);
+}

@@ -259,6 +259,67 @@ inch_status inch_spmm(int32_t prec, int64_t n_atoms, const int64_t* rowptr_dev,
                       void* ws_dev, size_t ws_bytes, cudaStream_t stream);
 
 /* ---------------------------------------------------------------------------
+ * Solver building blocks as single calls (for hosts that drive an iteration
+ * through this ABI).  Tall blocks are row-major (n rows, b columns, leading
+ * dimension ld >= b); n = 3 * n_atoms for the Hessian.  Every buffer, including
+ * scratch, is the caller's.
+ * ------------------------------------------------------------------------- */
+
+/* Y = sum_{k=0..degree} mu[k] T_k((H - cc)/dd) X on the store (prec 32 or 64),
+ * the three-term recurrence fused with its accumulation in each SpMM; W1, W2:
+ * work blocks of the same shape (leading dimension ldw).  X is not modified.
+ * Any b (column panels of 64 inside).  mu_host: degree + 1 host doubles.
+ * Replaces OOC2_A_Adiag_ChebyshevAv.ChebyshevAv (Burn/PolynomialFilters/T2.py:28-92). */
+inch_status inch_cheb_filter(int32_t prec, int64_t n_atoms, const int64_t* rowptr_dev, const void* ent_dev,
+                             const void* diag_dev, const void* X_dev, int64_t ldx, int32_t b, int32_t degree,
+                             const double* mu_host, double cc, double dd, void* Y_dev, int64_t ldy,
+                             void* W1_dev, void* W2_dev, int64_t ldw, cudaStream_t stream);
+
+/* Scaled Chebyshev filter of degree m damping [a, b_up], normalised at a0 < a
+ * (Zhou & Saad, J. Comput. Phys. 219 (2006)): Y = p_m(H) X; W: one work block.
+ * No reference counterpart (the block solver's filter; the reference filters one
+ * vector at a time through ChebyshevAv). */
+inch_status inch_cheb_filter_scaled(int32_t prec, int64_t n_atoms, const int64_t* rowptr_dev, const void* ent_dev,
+                                    const void* diag_dev, const void* X_dev, int64_t ldx, int32_t b, int32_t degree,
+                                    double a, double b_up, double a0, void* Y_dev, int64_t ldy, void* W_dev,
+                                    int64_t ldw, cudaStream_t stream);
+
+/* FP64 block orthonormalisation: Y <- Y - B^T (B Y) twice for each of the two
+ * optional row bases B1 (r1 x n, leading dimension ldb1) and B2 (locked modes,
+ * rigid-body basis), then `passes` Cholesky-QR passes (G = Y^T Y = L L^T,
+ * Y <- Y L^{-T}; a Gram matrix that is not numerically positive is retried once
+ * with a 1e-12 * max-diagonal shift; still not positive -> INCH_INVALID_ARG,
+ * "rank deficient").  cuBLAS runs the GEMMs and the triangular solve; its handle
+ * is created on a device's first call (cuBLAS's own small allocation), its GEMM
+ * workspace comes from ws.  Synchronises the stream once per pass.
+ * Replaces the Gram-Schmidt of Burn/Orthogonalization/T1.py:56-64 and
+ * T2.py:64-137 (one vector against the basis there, a whole block here). */
+size_t inch_block_orth_workspace_size(int32_t b, int64_t r_max);
+inch_status inch_block_orth(int64_t n, int32_t b, double* Y_dev, int64_t ldy, const double* B1_dev, int64_t r1,
+                            int64_t ldb1, const double* B2_dev, int64_t r2, int64_t ldb2, int32_t passes,
+                            void* ws_dev, size_t ws_bytes, cudaStream_t stream);
+
+/* Rayleigh-Ritz: G (b x b, symmetric, column-major) = sym(Y^T HY) for an
+ * orthonormal Y and HY = H Y (both FP64 blocks); and Z (n x m) = Y W for the m
+ * leading columns of the (column-major, b x b) eigenvector matrix W of G.  The
+ * small eigenproblem itself stays with the caller (LAPACK / cuSOLVER).
+ * Replaces the projected matrix of JacobiDavidsonHotellingDeflation/T1.py:440-451
+ * and the restart rotations of T1.py:662-666 / ThickRestartLanczos.../T1.py. */
+size_t inch_rr_workspace_size(void);
+inch_status inch_rr_project(int64_t n, int32_t b, const double* Y_dev, int64_t ldy, const double* HY_dev,
+                            int64_t ldh, double* G_dev, void* ws_dev, size_t ws_bytes, cudaStream_t stream);
+inch_status inch_rr_rotate(int64_t n, int32_t b, int32_t m, const double* Y_dev, int64_t ldy, const double* W_dev,
+                           double* Z_dev, int64_t ldz, void* ws_dev, size_t ws_bytes, cudaStream_t stream);
+
+/* res_dev[c] = || HY[:, c] - theta_dev[c] * Y[:, c] ||_2 in FP64 (deterministic
+ * two-stage reduction, no (n x b) temporary).
+ * Replaces the Ritz residual of JacobiDavidsonHotellingDeflation/T1.py:543-560. */
+size_t inch_residual_workspace_size(int32_t b);
+inch_status inch_residual_fp64(int64_t n, int32_t b, const double* HY_dev, int64_t ldh, const double* Y_dev,
+                               int64_t ldy, const double* theta_dev, double* res_dev, void* ws_dev,
+                               size_t ws_bytes, cudaStream_t stream);
+
+/* ---------------------------------------------------------------------------
  * Row-tile store for wide multivectors (no reference counterpart; an alternative
  * layout of the same matrix).  Atoms are grouped in tiles of 8 consecutive rows;
  * per tile, the merged sorted union of the rows' neighbour columns is stored as
