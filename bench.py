@@ -433,7 +433,7 @@ def run_shell(args):
     from inching_b200.hessian import HessianStore
     from inching_b200.learned import WarmStartMPNN, learned_warm_start
     from inching_b200.solvers.chfsi import chfsi_lean, default_guard
-    from inching_b200.warmstart import coarse_warm_start
+    from inching_b200.warmstart import coarse_warm_start, galerkin_warm_start
     k = 1000 if args.k == 256 else args.k
     p = k + default_guard(k)
     Xd = torch.from_numpy(synth.workload("shell500k") / 10.0).cuda()
@@ -454,6 +454,8 @@ def run_shell(args):
             X0 = coarse_warm_start(Xr, p)
         elif start == "learned_beads":
             X0, winfo = learned_warm_start(Xr, p, model, H.rowptr, H.cols, H=H, Q=Q, k=k, return_info=True)
+        elif start == "galerkin_beads":
+            X0 = galerkin_warm_start(H, p)
         ev, V, info = chfsi_lean(H, k, tol=args.tol, Q=Q, precision="mixed", X0=X0, return_info=True)
         e1.record()
         torch.cuda.synchronize()
@@ -469,7 +471,7 @@ def run_shell(args):
     res = {}
     evs = {}
     with Clocks(0) as clk:
-        for start in ("random", "uniform_beads", "learned_beads"):
+        for start in ("random", "uniform_beads", "learned_beads", "galerkin_beads"):
             res[start], evs[start] = solve(start)
             torch.cuda.empty_cache()
     agree = max(float(((evs[s] - evs["random"]).abs() / evs["random"]).max()) for s in evs)
@@ -480,6 +482,7 @@ def run_shell(args):
             "starts": res,
             "warm_start_gain_vs_random": round(res["random"]["seconds"] / res["learned_beads"]["seconds"], 2),
             "uniform_bead_gain_vs_random": round(res["random"]["seconds"] / res["uniform_beads"]["seconds"], 2),
+            "galerkin_bead_gain_vs_random": round(res["random"]["seconds"] / res["galerkin_beads"]["seconds"], 2),
             "max_eig_rel_diff_between_starts": agree,
             "peak_mem_gb": round(torch.cuda.max_memory_allocated() / 1e9, 1), "clocks": clk.summary()}
     print(json.dumps(line))

@@ -54,7 +54,9 @@ def normal_modes_device(X_nm: torch.Tensor, k: int, *, rc_gamma_A=8.0, plus_i=1.
     """Lowest k non-rigid modes of the structure X_nm (CUDA (N,3) float64, nm).
 
     warm_start="coarse" (block solver only): initial block from the lowest modes
-    of a bead model of the structure (inching_b200.warmstart); "learned": the bead
+    of a bead model of the structure (inching_b200.warmstart); "galerkin": from the
+    fine Hessian restricted to bead motions (P^T H P, the Rayleigh-Ritz-best bead
+    block); "learned": the bead
     model's spring constants set by the trained network (inching_b200.learned;
     warm_model= a WarmStartMPNN, default the shipped weights), with its residual
     test and random-start fallback.
@@ -86,6 +88,12 @@ def normal_modes_device(X_nm: torch.Tensor, k: int, *, rc_gamma_A=8.0, plus_i=1.
         from .warmstart import coarse_warm_start
         from .solvers.chfsi import default_guard
         kw["X0"], winfo = coarse_warm_start(Xr, k + default_guard(k), seed=seed, return_info=True)
+    elif warm_start == "galerkin":
+        if solver != "chfsi":
+            raise AssertionError("ABORTED. warm_start='galerkin' is available for solver='chfsi'")
+        from .warmstart import galerkin_warm_start
+        from .solvers.chfsi import default_guard
+        kw["X0"], winfo = galerkin_warm_start(H, k + default_guard(k), seed=seed, return_info=True)
     elif warm_start == "learned":
         if solver != "chfsi":
             raise AssertionError("ABORTED. warm_start='learned' is available for solver='chfsi'")
