@@ -58,3 +58,22 @@ def cpu_time_to_modes(X_nm, k, budget_s=15.0, tol_rel=1e-6, plain_iterations=Non
     if plain_iterations is not None:
         out["projected_s"] = t_pre + per_it * plain_iterations
     return out
+
+
+def arpack_time_to_modes(X_nm, k):
+    """The reference's own CPU baseline (Command8A/commandArpack_Pdb_0064_EPYC.py:
+    285-328): the Hessian's lower triangle symmetrised, then
+    scipy.sparse.linalg.eigsh(A, k, which='SA') -- no deflation, so the k + 6
+    lowest (six rigid-body modes at PlusI first).  Preprocessing as in
+    cpu_time_to_modes.  Returns (seconds, eigenvalues of the k non-rigid modes)."""
+    import scipy.sparse as sp
+    import scipy.sparse.linalg as sla
+    t0 = time.perf_counter()
+    deg, rowptr, cols = kdtree_neighbor_lists(X_nm)
+    order, _ = graph.cuthill_mckee(rowptr, cols, deg)
+    Xr = X_nm[order]
+    _, rp2, c2 = kdtree_neighbor_lists(Xr)
+    A, _ = hessian.hessian_lower(Xr, 8.0, 1.0, rowptr=rp2, cols=c2)
+    A_sym = (A + sp.tril(A, k=-1).T).tocsr()
+    w = sla.eigsh(A_sym, k=k + 6, which="SA", return_eigenvectors=False)
+    return time.perf_counter() - t0, np.sort(w)[6:]
