@@ -297,3 +297,30 @@ def test_pipeline_cdm():
     e1, m1, i1 = normal_modes_device(Xd, 12, solver="cdm", tol=1e-10, precision="mixed", block=4, degree=24)
     assert i1["converged"]
     assert float(((e1 - e0).abs() / e0).max()) < 1e-8
+
+
+def test_galerkin_bead_operator_and_start(small):
+    """The Galerkin bead operator equals M^-1/2 P^T H P M^-1/2 built densely from
+    the oracle Hessian, and the pipeline's Galerkin start converges to the same
+    eigenvalues as a cold start."""
+    import scipy.sparse as sp
+    from inching_b200.pipeline import normal_modes_device
+    from inching_b200.warmstart import GalerkinOperator, bead_model
+    s = small
+    H = s["H"]
+    _, bead = bead_model(H.X, 6.0)
+    nb = int(bead.max()) + 1
+    counts = torch.bincount(bead, minlength=nb)
+    G = GalerkinOperator(H, bead, nb, counts)
+    n = H.n_atoms
+    bd = bead.cpu().numpy()
+    P = sp.csr_matrix((np.ones(3 * n), (np.arange(3 * n), 3 * np.repeat(bd, 3) + np.tile([0, 1, 2], n))),
+                      shape=(3 * n, 3 * nb))
+    Mh = 1.0 / np.sqrt(np.repeat(counts.cpu().numpy(), 3).astype(float))
+    ref = sp.diags(Mh) @ (P.T @ sp.csr_matrix(s["Hd"]) @ P) @ sp.diags(Mh)
+    assert np.abs(G.csr64.to_dense().cpu().numpy() - ref.toarray()).max() < 1e-12 * np.abs(ref).max()
+    Xd = torch.from_numpy(s["Xr"]).cuda()
+    e0, _, _ = normal_modes_device(Xd, 24, tol=1e-9, precision="f64")
+    e1, _, i1 = normal_modes_device(Xd, 24, tol=1e-9, precision="f64", warm_start="galerkin")
+    assert i1["warm_start"]["beads"] == nb
+    assert float(((e1 - e0).abs() / e0).max()) < 1e-9
