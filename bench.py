@@ -58,6 +58,9 @@ def parse():
     ap.add_argument("--reps", type=int, default=5, help="launches for --kernel-only")
     ap.add_argument("--tune", default=None, help="threads,blocks_per_sm for the wide SpMM (--kernel-only)")
     ap.add_argument("--plain-lean", action="store_true", help="cube2400k: also time the FP64 block solve")
+    ap.add_argument("--degree", type=int, default=None, help="cube2400k: Chebyshev filter degree (default: the "
+                    "solver's size rule)")
+    ap.add_argument("--profile", action="store_true", help="cube2400k: CUDA-event phase times of the solver")
     ap.add_argument("--layout", default="tiles", choices=["tiles", "pairs"], help="store layout for --kernel-only")
     return ap.parse_args()
 
@@ -398,7 +401,8 @@ def run_largest(args):
         H = HessianStore(Xr, 8.0, 1.0, precisions=("f64", "f32") if precision == "mixed" else ("f64",))
         Q = rigid_body_basis(Xr)
         X0 = coarse_warm_start(Xr, k + default_guard(k)) if warm else None
-        ev, V, info = chfsi_lean(H, k, tol=args.tol, Q=Q, precision=precision, X0=X0, return_info=True)
+        ev, V, info = chfsi_lean(H, k, tol=args.tol, Q=Q, precision=precision, X0=X0, return_info=True,
+                                 degree=args.degree, profile=args.profile)
         del X0
         e1.record()
         torch.cuda.synchronize()
@@ -410,7 +414,8 @@ def run_largest(args):
             "steps": 1, "warmup": 0, "higher_is_better": False,
             "config": {"workload": "cube2400k: 2,400,000 atoms (300 touching globules of 8,000), 7.2M dof, "
                                    f"lowest {k} non-rigid modes", "solver": "memory-lean block ChFSI, mixed + warm"},
-            "max_rel_residual": info["max_rel_residual"], "iterations": info["iterations"],
+            "max_rel_residual": info["max_rel_residual"], "iterations": info["iterations"], "degree": info["degree"],
+            "phases_ms": info.get("phases_ms"),
             "peak_mem_gb": round(torch.cuda.max_memory_allocated() / 1e9, 1), "clocks": clk.summary()}
     if args.plain_lean:
         del ev

@@ -435,8 +435,24 @@ def _rows(n, rows):
         yield slice(r0, min(r0 + rows, n))
 
 
-def chfsi_lean(A, k, tol=1e-6, Q=None, precision="mixed", degree=24, guard=None, maxiter=100, X0=None, seed=0,
-               chunk=256, row_chunk=1 << 20, window=512, verbose=False, return_info=False):
+def lean_degree(A, p):
+    """Filter degree of the memory-lean solver: each iteration costs tall GEMMs
+    (~ n p^2, n dof) besides the filter's SpMMs (~ nnz p per degree, nnz stored
+    blocks), so the wider the block relative to the matrix, the more filtering per
+    iteration pays.  24 at p n / nnz <= 10 (256 modes of 100k atoms: 9.6), growing
+    with the square root of that ratio, in multiples of 8 up to 64 (1,000 modes of
+    2.4M atoms: ratio 37 -> 48, which took 4 iterations and 93 s against 10 and
+    126 s at 24)."""
+    nnz = getattr(A, "nnz_blocks", None)
+    if not nnz:
+        return 24
+    ratio = p * A.shape[0] / nnz          # dof x block width / stored blocks
+    d = 24.0 * math.sqrt(max(ratio, 10.0) / 10.0)
+    return int(min(64, max(24, 8 * round(d / 8))))
+
+
+def chfsi_lean(A, k, tol=1e-6, Q=None, precision="mixed", degree=None, guard=None, maxiter=100, X0=None, seed=0,
+               chunk=256, row_chunk=1 << 20, window=512, verbose=False, return_info=False, profile=False):
     """Same iteration as chfsi() with one (n, p) FP64 array B holding the locked
     modes (columns [0, L)) and the active block (columns [L, p)):
 
@@ -457,6 +473,8 @@ def chfsi_lean(A, k, tol=1e-6, Q=None, precision="mixed", degree=24, guard=None,
     if guard is None:
         guard = default_guard(k)
     p = min(k + guard, n - (0 if Q is None else Q.shape[0]))
+    if degree is None:
+        degree = lean_degree(A, p)
     Qd = None if Q is None else HessianOperator(A, Q=Q).Q
     lo, hi = estimate_spectrum_bound(A, steps=40, seed=seed + 1, precision=precision)
     b_up = hi * 1.02 + 1e-3 * abs(hi)
@@ -524,9 +542,13 @@ def chfsi_lean(A, k, tol=1e-6, Q=None, precision="mixed", degree=24, guard=None,
             res[cs:ce] = torch.linalg.vector_norm(R, dim=0).cpu().numpy()
         return th, res
 
-    project(0)
-    orth(0)
-    th, res = rayleigh_ritz(0)
+    ph = _Phases(profile)
+    with ph("project"):
+        project(0)
+    with ph("orth"):
+        orth(0)
+    with ph("rr"):
+        th, res = rayleigh_ritz(0)
     L = 0
     locked_theta = []
     filt = _Filter(A, prec)
@@ -549,7 +571,8 @@ def chfsi_lean(A, k, tol=1e-6, Q=None, precision="mixed", degree=24, guard=None,
         if stall >= STALL_RESTART and L:
             # locked + active Rayleigh-Ritz, as in chfsi(): clears the coupling of
             # the active block to modes locked inside a tight cluster
-            th, res = rayleigh_ritz(0)
+            with ph("rr"):
+                th, res = rayleigh_ritz(0)
             L = 0
             locked_theta = []
             stall = 0
@@ -559,12 +582,16 @@ def chfsi_lean(A, k, tol=1e-6, Q=None, precision="mixed", degree=24, guard=None,
         a0 = float(th[0])
         if not (a0 < a < b_up):
             a0 = a - 1e-3 * abs(a)
-        for cs in range(L, p, chunk):
-            ce = min(cs + chunk, p)
-            B[:, cs:ce] = filt(B[:, cs:ce], degree, a, b_up, a0 - 1e-12)
-        project(L)
-        orth(L)
-        th, res = rayleigh_ritz(L)
+        with ph("filter"):
+            for cs in range(L, p, chunk):
+                ce = min(cs + chunk, p)
+                B[:, cs:ce] = filt(B[:, cs:ce], degree, a, b_up, a0 - 1e-12)
+        with ph("project"):
+            project(L)
+        with ph("orth"):
+            orth(L)
+        with ph("rr"):
+            th, res = rayleigh_ritz(L)
     converged = L >= k
     # final FP64 Rayleigh-Ritz over the first k columns, explicit residuals
     Lk = B[:, :k]
@@ -587,5 +614,5 @@ def chfsi_lean(A, k, tol=1e-6, Q=None, precision="mixed", degree=24, guard=None,
     if return_info:
         return evals, V, dict(iterations=it + 1, converged=converged, n_spmm_filter=filt.n_spmm, block=p,
                               degree=degree, normH=b_up, max_rel_residual=worst, lock_restarts=n_restarts,
-                              seconds=time.perf_counter() - t_start)
+                              seconds=time.perf_counter() - t_start, phases_ms=ph.summary())
     return evals, V
