@@ -41,6 +41,16 @@ struct Ent<float> {
     wz = v.z;
     j = __float_as_int(v.w);
   }
+  // streaming load (evict-first): an entry read once per product should not push
+  // the gathered vector rows out of L1
+  __device__ __forceinline__ static void load_cs(const void* base, int64_t e, float& wx, float& wy, float& wz,
+                                                 int& j) {
+    float4 v = __ldcs(reinterpret_cast<const float4*>(base) + e);
+    wx = v.x;
+    wy = v.y;
+    wz = v.z;
+    j = __float_as_int(v.w);
+  }
 };
 template <>
 struct Ent<double> {
@@ -48,6 +58,15 @@ struct Ent<double> {
                                               int& j) {
     const double2* p = reinterpret_cast<const double2*>(base) + 2 * e;
     double2 a = __ldg(p), b = __ldg(p + 1);
+    wx = a.x;
+    wy = a.y;
+    wz = b.x;
+    j = static_cast<int>(b.y);
+  }
+  __device__ __forceinline__ static void load_cs(const void* base, int64_t e, double& wx, double& wy, double& wz,
+                                                 int& j) {
+    const double2* p = reinterpret_cast<const double2*>(base) + 2 * e;
+    double2 a = __ldcs(p), b = __ldcs(p + 1);
     wx = a.x;
     wy = a.y;
     wz = b.x;
@@ -81,10 +100,11 @@ k_spmm(int64_t n_atoms, const int64_t* __restrict__ rowptr, const void* __restri
 #pragma unroll
     for (int c = 0; c < B; ++c) acc[0][c] = acc[1][c] = acc[2][c] = T(0);
     const int64_t e1 = rowptr[i + 1];
+#pragma unroll 2
     for (int64_t e = rowptr[i] + lg; e < e1; e += G) {
       T wx, wy, wz;
       int j;
-      Ent<T>::load(ent, e, wx, wy, wz, j);
+      Ent<T>::load_cs(ent, e, wx, wy, wz, j);
       const T* xj = X + 3 * (int64_t)j * ldx + c0;
 #pragma unroll
       for (int c = 0; c < B; ++c) {
