@@ -72,7 +72,8 @@ def _bucket_warm_start(Xd, sid, n_struct, k, guard, seed, bead_edge_A=6.0, rc_be
 
 
 def batched_normal_modes(structs, k=32, *, units="nm", rc_gamma_A=8.0, plus_i=1.0, tol=1e-6, precision="mixed",
-                         degree=24, bucket_ratio=1.6, seed=0, verbose=False, profile=False, warm_start=None):
+                         degree=24, bucket_ratio=1.6, seed=0, verbose=False, profile=False, warm_start=None,
+                         guard=None):
     t0 = time.perf_counter()
     structs = [np.asarray(X, dtype=np.float64) / (10.0 if units == "A" else 1.0) for X in structs]
     if not structs:
@@ -105,7 +106,7 @@ def batched_normal_modes(structs, k=32, *, units="nm", rc_gamma_A=8.0, plus_i=1.
             torch.cuda.synchronize()
         tb1 = _t.perf_counter()
         ev, V, info = chfsi_batched(H, 3 * atom_off, k, tol=tol, Qp=Qp, precision=precision, degree=degree,
-                                    seed=seed, verbose=verbose, profile=profile, Y0=Y0)
+                                    seed=seed, verbose=verbose, profile=profile, Y0=Y0, guard=guard)
         if profile:
             torch.cuda.synchronize()
         tb2 = _t.perf_counter()

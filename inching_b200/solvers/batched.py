@@ -133,7 +133,12 @@ def chfsi_batched(H, dof_offsets, k, tol=1e-6, Qp=None, precision="mixed", degre
     S = seg.S
     prec = 32 if precision == "mixed" else 64
     if guard is None:
-        guard = max(16, int(math.ceil(0.5 * k)))
+        # at least max(16, k/2), then up to a multiple of 32 columns: the SpMM runs
+        # 32/64-column panels, so a block that fills them costs little more per step
+        # and converges in fewer (512 structures, k = 32: 64 columns, 3.0 s and at most
+        # 5 iterations per bucket, against 48 columns, 3.95 s and up to 8)
+        p0 = k + max(16, int(math.ceil(0.5 * k)))
+        guard = (p0 + 31) // 32 * 32 - k
     p = min(k + guard, int(seg.sizes.min()) - (0 if Qp is None else Qp.shape[1]))
     assert p > k, "ABORTED. a structure is too small for k modes plus guard vectors"
     with ph("bound"):
