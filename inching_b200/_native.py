@@ -78,6 +78,8 @@ _SIGS = {
     "inch_residual_workspace_size": (c_size_t, [c_int32]),
     "inch_residual_fp64": (ctypes.c_int, [c_int64, c_int32, c_void_p, c_int64, c_void_p, c_int64, c_void_p, c_void_p,
                                           c_void_p, c_size_t, c_void_p]),
+    "inch_eigh_batched_small": (ctypes.c_int, [c_void_p, c_int64, c_int32, c_void_p, c_void_p, c_int32, c_double,
+                                               c_void_p, c_void_p]),
     "inch_hessian_assemble_pbc_xy": (ctypes.c_int, [c_void_p, c_int64, c_double, c_double, c_void_p, c_void_p,
                                                     c_void_p, c_double, c_double, c_void_p, c_void_p, c_void_p,
                                                     c_void_p, c_void_p]),
@@ -488,3 +490,16 @@ def residual_fp64(HY, Y, theta):
                                _ptr(ws), ws.numel(), _stream()))
     _count(2)
     return res
+
+
+def eigh_batched_small(G, max_sweeps=30, tol=1e-13, return_sweeps=False):
+    """Eigenpairs of a (S, p, p) stack of symmetric FP64 device matrices, p <= 64:
+    (W (S, p) ascending, V (S, p, p) eigenvectors in columns), one CTA per matrix."""
+    _require_cuda(G, "G", torch.float64)
+    S, p, _ = G.shape
+    W = torch.empty((S, p), dtype=torch.float64, device=G.device)
+    V = torch.empty((S, p, p), dtype=torch.float64, device=G.device)
+    sw = torch.empty(S, dtype=torch.int32, device=G.device) if return_sweeps else None
+    check(lib().inch_eigh_batched_small(_ptr(G), S, p, _ptr(W), _ptr(V), max_sweeps, tol, _ptr(sw), _stream()))
+    _count(1)
+    return (W, V, sw) if return_sweeps else (W, V)

@@ -319,6 +319,16 @@ inch_status inch_residual_fp64(int64_t n, int32_t b, const double* HY_dev, int64
                                int64_t ldy, const double* theta_dev, double* res_dev, void* ws_dev,
                                size_t ws_bytes, cudaStream_t stream);
 
+/* Eigenpairs of n_mat symmetric p x p FP64 matrices (row-major, one after the
+ * other; p <= 64): W (n_mat, p) ascending, V (n_mat, p, p) with eigenvector k in
+ * column k.  One CTA per matrix, cyclic Jacobi in shared memory, sweeps until the
+ * off-diagonal norm is below tol times the matrix's or max_sweeps (<= 100; the
+ * count used per matrix goes to sweeps_used if not NULL).  No reference
+ * counterpart: the small projected eigenproblems of the batched solve (one per
+ * structure), which the reference would solve one at a time with numpy. */
+inch_status inch_eigh_batched_small(const double* A_dev, int64_t n_mat, int32_t p, double* W_dev, double* V_dev,
+                                    int32_t max_sweeps, double tol, int32_t* sweeps_used_dev, cudaStream_t stream);
+
 /* ---------------------------------------------------------------------------
  * Row-tile store for wide multivectors (no reference counterpart; an alternative
  * layout of the same matrix).  Atoms are grouped in tiles of 8 consecutive rows;

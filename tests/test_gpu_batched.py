@@ -4,6 +4,7 @@ Tolerances: mixed precision at residual 1e-6*||H|| -> relative eigenvalue error
 <= 1e-6; FP64 at 1e-9*||H|| -> 1e-10."""
 import numpy as np
 import pytest
+import torch
 
 from oracle import hessian as oh
 
@@ -72,3 +73,28 @@ def test_sharded_batch_in_one_process_equals_batched():
         ev2, m2 = merged[i]
         assert np.max(np.abs(ev2 - ev) / ev) < 1e-9
         assert m2.shape == tuple(modes.shape)
+
+
+@pytest.mark.parametrize("p", [1, 2, 37, 48, 64])
+def test_jacobi_batched_small_eigh(p):
+    """The batched Jacobi kernel against LAPACK on random symmetric matrices and on
+    ones with a repeated eigenvalue: eigenvalues to 1e-12 of the norm, orthonormal
+    eigenvectors, residual A V - V W to 1e-12 of the norm."""
+    from inching_b200 import _native
+    rng = np.random.default_rng(p)
+    A = rng.standard_normal((40, p, p))
+    A = A + A.transpose(0, 2, 1)
+    Q, _ = np.linalg.qr(rng.standard_normal((p, p)))
+    d = np.arange(p, dtype=float) // 2           # pairs of equal eigenvalues
+    A[0] = (Q * d) @ Q.T
+    G = torch.from_numpy(A).cuda()
+    W, V, sw = _native.eigh_batched_small(G, return_sweeps=True)
+    W, V = W.cpu().numpy(), V.cpu().numpy()
+    w_ref = np.linalg.eigvalsh(A)
+    nrm = np.abs(A).max()
+    assert np.abs(W - w_ref).max() < 1e-12 * nrm * p
+    I = np.eye(p)
+    assert np.abs(np.einsum("sji,sjk->sik", V, V) - I).max() < 1e-12 * p
+    R = np.einsum("sij,sjk->sik", A, V) - V * W[:, None, :]
+    assert np.abs(R).max() < 1e-12 * nrm * p
+    assert int(sw.max()) <= 30
