@@ -123,6 +123,16 @@ def _project_b(P, Qp):
     return P
 
 
+def batched_guard(k):
+    """Guard vectors of the batched solve: at least max(16, k/2), then up to a
+    multiple of 32 columns.  The SpMM runs 32/64-column panels, so a block that
+    fills them costs little more per step and converges in fewer (512 structures,
+    k = 32: 64 columns, 3.0 s and at most 5 iterations per bucket, against 48
+    columns, 3.95 s and up to 8)."""
+    p0 = k + max(16, int(math.ceil(0.5 * k)))
+    return (p0 + 31) // 32 * 32 - k
+
+
 def chfsi_batched(H, dof_offsets, k, tol=1e-6, Qp=None, precision="mixed", degree=24, guard=None, maxiter=200,
                   seed=0, verbose=False, profile=False, Y0=None):
     """Lowest k modes (orthogonal to Qp) of every diagonal block of H.
@@ -138,12 +148,7 @@ def chfsi_batched(H, dof_offsets, k, tol=1e-6, Qp=None, precision="mixed", degre
     S = seg.S
     prec = 32 if precision == "mixed" else 64
     if guard is None:
-        # at least max(16, k/2), then up to a multiple of 32 columns: the SpMM runs
-        # 32/64-column panels, so a block that fills them costs little more per step
-        # and converges in fewer (512 structures, k = 32: 64 columns, 3.0 s and at most
-        # 5 iterations per bucket, against 48 columns, 3.95 s and up to 8)
-        p0 = k + max(16, int(math.ceil(0.5 * k)))
-        guard = (p0 + 31) // 32 * 32 - k
+        guard = batched_guard(k)
     p = min(k + guard, int(seg.sizes.min()) - (0 if Qp is None else Qp.shape[1]))
     assert p > k, "ABORTED. a structure is too small for k modes plus guard vectors"
     with ph("bound"):

@@ -1,0 +1,139 @@
+"""Host-side logic of the solvers, on CPU: the degree and guard rules, the filter
+coefficient tables, the periodic-box parser, and the control flow of the
+per-column filter and of the Chebyshev-Davidson and block solvers run against a
+dense CPU test double of the Hessian store (the product itself needs CUDA)."""
+import numpy as np
+import pytest
+import torch
+
+from oracle import hessian as oh
+
+
+class DenseStore:
+    """Test double with the store's matmul interface (fused epilogue) on a dense
+    CPU matrix."""
+
+    def __init__(self, H):
+        self.Hd = torch.from_numpy(np.asarray(H))
+        self.shape = self.Hd.shape
+        self.device = torch.device("cpu")
+        self.ndim = 2
+        self.dtype = torch.float64
+
+    def matmul(self, X, out=None, prec=64, alpha=1.0, gamma=0.0, beta=0.0, Yin=None, acc=None, mu=0.0, Q=None,
+               hot_shift=0.0):
+        H = self.Hd.to(X.dtype)
+        Y = alpha * (H @ X) + gamma * X
+        if Yin is not None:
+            Y = Y + beta * Yin
+        if Q is not None and hot_shift:
+            q = Q.to(X.dtype)
+            Y = Y + hot_shift * (q.t() @ (q @ X))
+        if acc is not None:
+            acc += mu * Y
+        if out is not None:
+            out.copy_(Y)
+            return out
+        return Y
+
+
+@pytest.fixture(scope="module")
+def dense():
+    from inching_b200 import synth
+    X = synth.globule(300, seed=3) / 10.0
+    A, Ad = oh.hessian_lower(X, 8.0, 1.0)
+    H = oh.full_from_lower(A, Ad).toarray()
+    w, U = np.linalg.eigh(H)
+    Q = torch.from_numpy(oh.rigid_body_basis(X))
+    return dict(F=DenseStore(H), w=w, U=U, Q=Q)
+
+
+def test_lean_degree_rule():
+    from inching_b200.solvers.chfsi import lean_degree
+
+    class S:
+        pass
+
+    def deg(n_atoms, nnz, p):
+        a = S()
+        a.shape = (3 * n_atoms, 3 * n_atoms)
+        a.nnz_blocks = nnz
+        return lean_degree(a, p)
+
+    assert deg(100000, 10064346, 320) == 24          # the 100k-atom configuration
+    assert deg(2400000, 241e6, 1250) == 48           # 1,000 modes of 2.4M atoms
+    assert deg(498000, 51e6, 1250) == 48
+    assert deg(10**7, 1e9, 5000) == 64               # capped
+    assert lean_degree(S(), 100) == 24               # an operator without a block count
+
+
+def test_batched_guard_rounds_to_panels():
+    from inching_b200.solvers.batched import batched_guard
+    assert batched_guard(32) == 32 and (32 + batched_guard(32)) % 32 == 0
+    for k in (1, 8, 12, 33, 64, 100):
+        g = batched_guard(k)
+        assert g >= max(16, int(np.ceil(k / 2))) and (k + g) % 32 == 0
+
+
+def test_chebyshev_degrees():
+    from inching_b200.solvers.chfsi import chebyshev_degrees
+    theta = np.array([1.2, 2.0, 4.9, 5.0, 7.0])
+    res = np.array([1e-3, 1e-5, 1e-2, 1.0, 1.0])
+    d = chebyshev_degrees(theta, res, 3, 1e-6, 5.0, 60.0, 24)
+    assert list(d[3:]) == [24, 24]                    # guard vectors keep the full degree
+    assert d[1] < d[0] <= 24 and d[2] == 24           # closer to converged, further from a: fewer steps
+    assert (d >= 2).all()
+
+
+def test_cdm_filter_rows_are_chebyshev():
+    from inching_b200.solvers.cdm import filter_rows
+    low, high, m = 3.0, 40.0, 9
+    rows = filter_rows(m, low, high)
+    e, c = (high - low) / 2, (high + low) / 2
+    for lam in (0.5, 2.9, 10.0, 39.0):
+        x0 = 1.0
+        a0, g0, _ = rows[0]
+        x1 = a0 * lam * x0 + g0 * x0
+        prev, cur = x0, x1
+        for a, g, b in rows[1:]:
+            prev, cur = cur, a * lam * cur + g * cur + b * prev
+        ref = np.polynomial.chebyshev.chebval((c - lam) / e, [0] * (m + 1) + [1])
+        assert cur == pytest.approx(ref, rel=1e-10)
+
+
+def test_pbc_box_parser():
+    from inching_b200.graph import pbc_box
+    assert pbc_box(None) is None
+    assert pbc_box({"RectBox_Xsize": 3.5, "RectBox_Ysize": 2.0, "RectBox_Zsize": 9.0}) == (3.5, 2.0)
+    assert pbc_box((1, 2)) == (1.0, 2.0)
+
+
+def test_per_column_filter_equals_single_degree_runs(dense):
+    from inching_b200.solvers.chfsi import _Filter
+    f = _Filter(dense["F"], 64)
+    X = torch.randn(dense["F"].shape[0], 13, dtype=torch.float64, generator=torch.Generator().manual_seed(1))
+    degs = np.random.default_rng(0).integers(1, 10, size=13)
+    a, b, a0 = 5.0, dense["w"][-1] * 1.02, dense["w"][0]
+    Z = f(X, 9, a, b, a0, degrees=degs)
+    for i in range(13):
+        zi = f(X[:, i:i + 1].contiguous(), int(degs[i]), a, b, a0)
+        assert torch.allclose(zi[:, 0], Z[:, i], rtol=0, atol=1e-12 * float(zi.abs().max()))
+
+
+@pytest.mark.parametrize("block,with_q", [(1, False), (1, True), (4, True)])
+def test_cdm_control_flow_on_dense_double(dense, block, with_q):
+    from inching_b200.solvers.cdm import cdm
+    w = dense["w"]
+    S, V, info = cdm(dense["F"], 12, tol=1e-10, degree=12, spectrum_bound=(w[0], w[-1]), cuda_graph=False,
+                     Q=dense["Q"] if with_q else None, block=block, return_info=True)
+    off = 6 if with_q else 0
+    assert info["converged"]
+    assert np.abs(S.numpy() - w[off:off + 12]).max() < 1e-9 * w[-1]
+
+
+def test_block_solver_control_flow_on_dense_double(dense):
+    from inching_b200.solvers.chfsi import chfsi
+    w = dense["w"]
+    S, V, info = chfsi(dense["F"], 20, tol=1e-9, Q=dense["Q"], precision="f64", return_info=True)
+    assert info["converged"] and info["max_rel_residual"] <= 1.5e-9
+    assert np.abs(S.numpy() - w[6:26]).max() < 1e-8 * w[-1]
