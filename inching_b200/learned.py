@@ -295,6 +295,8 @@ def learned_warm_start(X_nm: torch.Tensor, n_vectors: int, model: WarmStartMPNN,
                        bead_edge_A=6.0, rc_bead_A=12.0, tol=1e-4, H=None, Q=None, k=None, seed=0,
                        return_info=False):
     """(3N, n_vectors) FP64 initial block from the learned bead model's lowest modes.
+    With k (the wanted fine modes), only the k lowest bead modes are converged and
+    the rest of the block is the coarse solver's guard Ritz vectors.
 
     With the fine Hessian store H (and its rigid basis Q), the block must pass the
     residual test: over the leading TEST_COLUMNS columns (the lowest bead modes),
@@ -312,7 +314,9 @@ def learned_warm_start(X_nm: torch.Tensor, n_vectors: int, model: WarmStartMPNN,
     if bool(torch.isfinite(gamma).all()):
         Hb = HessianStore(G.pos, rc_bead_A, plus_i=1.0, graph_=(G.degree, G.rowptr, G.cols),
                           pair_weight=G.adjacency_weights(gamma))
-        _, Vc = chfsi(Hb, m, tol=tol, Q=rigid_body_basis(G.pos), precision="mixed", seed=seed + 7)
+        kc = m if k is None else max(1, min(int(k), m))    # as in warmstart.coarse_warm_start(wanted=k)
+        _, Vc = chfsi(Hb, kc, tol=tol, Q=rigid_body_basis(G.pos), precision="mixed", seed=seed + 7,
+                      guard=m - kc if kc < m else None, final_f64=False, return_block=kc < m)
         V = Vc.reshape(G.n, 3, m).index_select(0, G.bead).reshape(3 * X_nm.shape[0], m)
         if m < n_vectors:
             V = torch.cat([V, torch.randn((V.shape[0], n_vectors - m), generator=gen, dtype=V.dtype,

@@ -88,8 +88,10 @@ def normal_modes_device(X_nm: torch.Tensor, k: int, *, rc_gamma_A=8.0, plus_i=1.
         from .warmstart import coarse_warm_start
         from .solvers.chfsi import default_guard
         # the starting block needs no tight coarse solve: tol 3e-3 kept the fine
-        # iterations of 256 modes of 100k atoms at 4 and saved 10 ms against 1e-4
-        kw["X0"], winfo = coarse_warm_start(Xr, k + default_guard(k), tol=3e-3, seed=seed, return_info=True)
+        # iterations of 256 modes of 100k atoms at 4 and saved 10 ms against 1e-4;
+        # only the k wanted bead modes converge, the guard columns stay Ritz vectors
+        kw["X0"], winfo = coarse_warm_start(Xr, k + default_guard(k), tol=3e-3, seed=seed, return_info=True,
+                                            wanted=k)
     elif warm_start == "galerkin":
         if solver != "chfsi":
             raise AssertionError("ABORTED. warm_start='galerkin' is available for solver='chfsi'")

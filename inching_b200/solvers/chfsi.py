@@ -304,12 +304,15 @@ class _Span:
 
 def chfsi(A, k, tol=1e-6, Q=None, precision="mixed", degree=24, guard=None, maxiter=300, X0=None, seed=0,
           spectrum_upper=None, final_f64=True, verbose=False, return_info=False, profile=False, cuda_graph=False,
-          adaptive_degree=False):
+          adaptive_degree=False, return_block=False):
     """Lowest k eigenpairs of A (+PlusI) orthogonal to the rows of Q.
 
     tol is relative: a pair is locked when ||H y - theta y|| <= tol * ||H||, with
     ||H|| estimated by the Lanczos upper bound of the spectrum.
-    Returns (eigenvalues (k,) ascending, eigenvectors (n, k)) as FP64 CUDA tensors."""
+    Returns (eigenvalues (k,) ascending, eigenvectors (n, k)) as FP64 CUDA tensors.
+    With return_block, the eigenvector array is the whole (n, k + guard) block:
+    the k locked modes followed by the unconverged Ritz vectors of the last
+    Rayleigh-Ritz step, all orthonormal (an initial block for a finer solve)."""
     t_start = time.perf_counter()
     n = A.shape[0]
     dev = A.device
@@ -415,6 +418,11 @@ def chfsi(A, k, tol=1e-6, Q=None, precision="mixed", degree=24, guard=None, maxi
         evals = evals[idx]
         L = L[:, torch.from_numpy(idx).to(dev)]
         final_res = None
+    if return_block:
+        # the active block holds p - (modes locked before the exit) columns; after a
+        # non-converged exit its leading ones were appended to the locked set, so the
+        # unused Ritz vectors are always its trailing p - k columns
+        L = torch.cat([L, Y[:, Y.shape[1] - (p - k):]], dim=1)
     evals_t = torch.from_numpy(np.ascontiguousarray(evals)).to(dev)
     if return_info:
         info = dict(iterations=it + 1, converged=converged, n_spmm_filter=filt.n_spmm, n_rr=n_rr,

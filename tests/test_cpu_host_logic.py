@@ -137,3 +137,23 @@ def test_block_solver_control_flow_on_dense_double(dense):
     S, V, info = chfsi(dense["F"], 20, tol=1e-9, Q=dense["Q"], precision="f64", return_info=True)
     assert info["converged"] and info["max_rel_residual"] <= 1.5e-9
     assert np.abs(S.numpy() - w[6:26]).max() < 1e-8 * w[-1]
+
+
+@pytest.mark.parametrize("maxiter", [300, 1])
+def test_block_solver_returns_whole_orthonormal_block(dense, maxiter):
+    """return_block: the k locked modes followed by the guard's Ritz vectors, all
+    orthonormal and orthogonal to the deflated rows, after a converged exit and
+    after one that stopped at maxiter."""
+    import torch
+    from inching_b200.solvers.chfsi import chfsi
+    w = dense["w"]
+    S, B, info = chfsi(dense["F"], 20, tol=1e-9, Q=dense["Q"], precision="f64", guard=12, maxiter=maxiter,
+                       return_block=True, return_info=True)
+    assert B.shape == (dense["F"].shape[0], 32) and S.shape == (20,)
+    assert info["converged"] == (maxiter == 300)
+    eye = torch.eye(32, dtype=torch.float64)
+    assert (B.t() @ B - eye).abs().max() < 1e-10
+    Q = torch.as_tensor(dense["Q"], dtype=torch.float64)
+    assert (Q @ B).abs().max() < 1e-10
+    if info["converged"]:
+        assert np.abs(S.numpy() - w[6:26]).max() < 1e-8 * w[-1]

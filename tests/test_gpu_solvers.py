@@ -324,3 +324,40 @@ def test_galerkin_bead_operator_and_start(small):
     e1, _, i1 = normal_modes_device(Xd, 24, tol=1e-9, precision="f64", warm_start="galerkin")
     assert i1["warm_start"]["beads"] == nb
     assert float(((e1 - e0).abs() / e0).max()) < 1e-9
+
+
+def test_coarse_bead_start_block_and_pipeline(small):
+    """coarse_warm_start(wanted=k): the block holds the k converged bead modes then
+    the coarse solver's guard Ritz vectors, every column a prolonged bead motion
+    (equal rows for the atoms of a bead) whose bead-space block is orthonormal and
+    orthogonal to the bead rigid-body motions; the leading k meet the coarse
+    tolerance on the bead Hessian.  The pipeline's coarse start converges to the cold start's eigenvalues."""
+    from inching_b200.deflation import rigid_body_basis
+    from inching_b200.hessian import HessianStore
+    from inching_b200.pipeline import normal_modes_device
+    from inching_b200.spectrum import estimate_spectrum_bound
+    from inching_b200.warmstart import bead_model, coarse_warm_start
+    s = small
+    Xd = torch.from_numpy(s["Xr"]).cuda()
+    pos, bead = bead_model(Xd, 6.0)
+    nb, k, width, tol = pos.shape[0], 24, 40, 3e-3
+    V, info = coarse_warm_start(Xd, width, tol=tol, wanted=k, return_info=True)
+    assert V.shape == (Xd.shape[0] * 3, width) and info["coarse_converged"] == k
+    Vb = V.reshape(-1, 3, width)
+    # one atom per bead (any: the rows of a bead's atoms are equal) gives back the bead block
+    first = torch.zeros(nb, dtype=torch.long, device=Xd.device).scatter_(0, bead, torch.arange(len(bead),
+                                                                                               device=Xd.device))
+    Z = Vb[first].reshape(3 * nb, width)
+    assert (Vb - Vb[first][bead]).abs().max() == 0
+    assert (Z.t() @ Z - torch.eye(width, dtype=Z.dtype, device=Z.device)).abs().max() < 1e-10
+    assert (rigid_body_basis(pos) @ Z).abs().max() < 1e-10
+    Hc = HessianStore(pos, 12.0, plus_i=1.0)
+    HZ = Hc.matmul(Z[:, :k].contiguous(), prec=64)
+    th = (Z[:, :k] * HZ).sum(dim=0)
+    res = torch.linalg.vector_norm(HZ - Z[:, :k] * th[None, :], dim=0)
+    _, hi = estimate_spectrum_bound(Hc, steps=40, seed=1)
+    assert float(res.max()) <= tol * 1.05 * hi
+    e0, _, _ = normal_modes_device(Xd, k, tol=1e-9, precision="f64")
+    e1, _, i1 = normal_modes_device(Xd, k, tol=1e-9, precision="f64", warm_start="coarse")
+    assert i1["warm_start"]["coarse_converged"] == k
+    assert float(((e1 - e0).abs() / e0).max()) < 1e-9
