@@ -23,9 +23,9 @@ Communication.
 
 The per-rank work is the single-GPU solver's with the matrix and the block cut
 by rows, and the results equal the single-GPU solver's to the solver tolerance
-(the random start differs).  The Chebyshev recurrence's epilogue (alpha H X +
-gamma X + beta Yin, accumulate) is applied to the owned rows after the local
-product instead of inside the SpMM kernel.
+(the random start differs).  The Chebyshev filter keeps its two recurrence
+buffers at the size of the extended range, so the recurrence's epilogue
+(alpha H X + gamma X + beta Yin) stays fused in the SpMM as on one GPU.
 """
 from __future__ import annotations
 
@@ -36,7 +36,7 @@ import numpy as np
 import torch
 import torch.distributed as dist
 
-from .solvers.chfsi import STALL_RESTART, _Filter, default_guard
+from .solvers.chfsi import STALL_RESTART, default_guard
 
 
 # ---------------------------------------------------------------------------
@@ -143,7 +143,8 @@ class RowBlockComm:
 class StoreRows:
     """Rows [a, b) of the Hessian store with columns rebased to [lo, hi), built by
     the package's neighbour lists and assembly kernels: a store over the atoms
-    [lo, hi) whose halo atoms have no entries (their product rows are dropped)."""
+    [lo, hi) whose halo atoms have no entries, so a product's halo rows carry no
+    H term (callers overwrite or drop them)."""
 
     def __init__(self, X_nm, rc_gamma_A, plus_i, rowptr, cols, a, b, lo, hi, precisions=("f64", "f32")):
         from .hessian import HessianStore
@@ -160,7 +161,13 @@ class StoreRows:
         self.own = slice(3 * (a - lo), 3 * (b - lo))
         self.nnz_blocks = e1 - e0
 
+    def ext_matmul(self, X_ext, out, prec, **epilogue):
+        """out = alpha H_rows X_ext + gamma X_ext + beta Yin (+ acc) over all rows of
+        the extended range, in one fused SpMM (the single-GPU store's epilogue)."""
+        return self.store.matmul(X_ext, out=out, prec=prec, **epilogue)
+
     def local_matmul(self, X_ext, prec):
+        """This rank's rows of H X_ext."""
         return self.store.matmul(X_ext, prec=prec)[self.own]
 
 
@@ -192,8 +199,9 @@ class RowBlockOperator:
     (3 (b - a), w) and returns its rows of alpha H X + gamma X + beta Yin (+ acc),
     the interface of the single-GPU store, after one halo exchange.
 
-    local: object with local_matmul(X_ext, prec) -> this rank's rows of H X_ext,
-    X_ext holding the atoms [lo, hi)."""
+    local: object with ext_matmul(X_ext, out, prec, alpha=, gamma=, beta=, Yin=)
+    computing alpha H_rows X_ext + gamma X_ext + beta Yin over every row of the
+    extended range [lo, hi) (StoreRows; the halo rows have no H term)."""
 
     def __init__(self, local, parts, ranges, comm: RowBlockComm, n_atoms, device):
         self.local = local
@@ -214,13 +222,23 @@ class RowBlockOperator:
         if int(comm.allreduce_(tot).item()) != self.shape[0]:
             raise AssertionError("ABORTED. the row blocks do not cover the structure")
 
-    def _ext(self, X):
+    @property
+    def n_ext(self):
+        """Dof rows of the extended range [lo, hi)."""
+        return 3 * (self.lay.hi - self.lay.lo)
+
+    @property
+    def own(self):
+        """This rank's rows within the extended range."""
+        off = 3 * (self.lay.a - self.lay.lo)
+        return slice(off, off + self.n_local)
+
+    def exchange_(self, Xe):
+        """Refresh the halo rows of an extended block Xe (3 (hi - lo), w) in place
+        from the peers' own rows; Xe's own rows are sent to the peers that need
+        them.  Every message is a contiguous row slab of Xe."""
         lay = self.lay
-        shape = (3 * (lay.hi - lay.lo),) + tuple(X.shape[1:])
-        Xe = torch.empty(shape, dtype=X.dtype, device=X.device)
-        off = 3 * (lay.a - lay.lo)
-        Xe[off:off + X.shape[0]] = X
-        snd = [(p, X[3 * (u - lay.a):3 * (v - lay.a)].contiguous()) for p, u, v in self.sends]
+        snd = [(p, Xe[3 * (u - lay.lo):3 * (v - lay.lo)]) for p, u, v in self.sends]
         rcv = [(p, Xe[3 * (u - lay.lo):3 * (v - lay.lo)]) for p, u, v in self.recvs]
         self.comm.p2p(snd, rcv)
         self.halo_bytes += sum(t.numel() * t.element_size() for _, t in rcv)
@@ -231,7 +249,11 @@ class RowBlockOperator:
             raise AssertionError("ABORTED. the row-block operator deflates by projection, not by a Hotelling term")
         if prec is None:
             prec = 64 if X.dtype == torch.float64 else 32
-        Y = self.local.local_matmul(self._ext(X.contiguous()), prec)
+        Xe = torch.empty((self.n_ext,) + tuple(X.shape[1:]), dtype=X.dtype, device=X.device)
+        Xe[self.own] = X
+        Ye = torch.empty_like(Xe)
+        self.local.ext_matmul(self.exchange_(Xe), Ye, prec)
+        Y = Ye[self.own]
         self.n_spmm += 1
         if alpha != 1.0:
             Y = Y * alpha
@@ -245,6 +267,47 @@ class RowBlockOperator:
             return Y
         out.copy_(Y)
         return out
+
+
+class _RowFilter:
+    """The scaled Chebyshev filter of solvers.chfsi._Filter on extended blocks:
+    the recurrence's two buffers hold the atoms [lo, hi); before each product the
+    halo rows of the vector being multiplied are refreshed from the peers, and
+    the recurrence's epilogue (alpha, gamma, beta Yin) runs inside the local
+    SpMM over all extended rows.  A result's halo rows (no H term) are
+    overwritten by the next exchange before any product reads them, and the
+    epilogue is row-local, so the own rows are exact."""
+
+    def __init__(self, A: "RowBlockOperator", prec):
+        self.A = A
+        self.prec = prec
+        self.n_spmm = 0
+
+    def __call__(self, X64, m, a, b, a0):
+        A = self.A
+        dt = torch.float64 if self.prec == 64 else torch.float32
+        e = (b - a) / 2.0
+        c = (b + a) / 2.0
+        sigma = e / (a0 - c)
+        sigma1 = sigma
+        tau = 2.0 / sigma1
+        w = X64.shape[1]
+        wp = (w + 7) // 8 * 8          # aligned width for the vector-gather SpMM
+        X = torch.zeros((A.n_ext, wp), dtype=dt, device=X64.device)
+        X[A.own, :w] = X64
+        Y = torch.empty_like(X)
+        A.local.ext_matmul(A.exchange_(X), Y, self.prec, alpha=sigma1 / e, gamma=-sigma1 * c / e)
+        self.n_spmm += 1
+        for _ in range(2, m + 1):
+            s2 = 1.0 / (tau - sigma)
+            # X <- 2 s2/e (H Y - c Y) - sigma s2 X, written over X, then swap
+            A.local.ext_matmul(A.exchange_(Y), X, self.prec, alpha=2.0 * s2 / e, gamma=-2.0 * s2 * c / e,
+                               beta=-sigma * s2, Yin=X)
+            X, Y = Y, X
+            sigma = s2
+            self.n_spmm += 1
+        A.n_spmm += self.n_spmm
+        return Y[A.own, :w].to(torch.float64)
 
 
 # ---------------------------------------------------------------------------
@@ -378,7 +441,7 @@ def chfsi_rowblock(A: RowBlockOperator, k, tol=1e-6, Q=None, precision="mixed", 
     Y = torch.randn((n_loc, p), generator=g, dtype=torch.float64, device=dev)
     Y = _cholqr(comm, _project_out(comm, Y, Qd), n)
     th, Y, HY = _rr(comm, A, Y, prec)
-    filt = _Filter(A, prec)
+    filt = _RowFilter(A, prec)
     locked = torch.empty((0, n_loc), dtype=torch.float64, device=dev)
     locked_theta = []
     it, n_rr, n_restarts, stall = 0, 1, 0, 0

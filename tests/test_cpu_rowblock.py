@@ -30,14 +30,25 @@ def _structure(n_atoms=400, seed=5):
 
 
 class DenseRows:
-    """Rows [a, b) of a dense H restricted to the columns of atoms [lo, hi)."""
+    """Rows [a, b) of a dense H restricted to the columns of atoms [lo, hi), with
+    the store's ext_matmul interface: the epilogue over every extended row, the
+    halo rows without an H term."""
 
     def __init__(self, H, a, b, lo, hi):
         self.H64 = torch.from_numpy(np.ascontiguousarray(H[3 * a:3 * b, 3 * lo:3 * hi]))
         self.H32 = self.H64.float()
+        self.own = slice(3 * (a - lo), 3 * (b - lo))
 
-    def local_matmul(self, X_ext, prec):
-        return (self.H64 if prec == 64 else self.H32) @ X_ext
+    def ext_matmul(self, X_ext, out, prec, alpha=1.0, gamma=0.0, beta=0.0, Yin=None, acc=None, mu=0.0):
+        Y = torch.zeros_like(X_ext)
+        Y[self.own] = (self.H64 if prec == 64 else self.H32) @ X_ext
+        Y = alpha * Y + gamma * X_ext
+        if Yin is not None and beta != 0.0:
+            Y = Y + beta * Yin
+        if acc is not None:
+            acc += mu * Y
+        out.copy_(Y)
+        return out
 
 
 def test_partition_halo_and_exchange_plan():
