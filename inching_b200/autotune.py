@@ -30,9 +30,28 @@ def _apply(H, cfg):
     H.use_tiles = layout == "tiles"
 
 
-def tune_spmm(H, b, prec=32, reps=3, candidates=CANDIDATES):
-    """Pick and apply the fastest configuration for (H, b, prec); returns (cfg, ms table)."""
-    key = (H.n_atoms, H.nnz_blocks, _width_class(b), prec, torch.cuda.get_device_name())
+def cuda_event_ms(fn, reps):
+    """Fastest of `reps` runs of fn in ms, CUDA events on the current stream, after
+    one untimed run."""
+    fn()
+    ev = [(torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)) for _ in range(reps)]
+    for e0, e1 in ev:
+        e0.record()
+        fn()
+        e1.record()
+    torch.cuda.synchronize()
+    return min(e0.elapsed_time(e1) for e0, e1 in ev)
+
+
+def _device_name(dev):
+    dev = torch.device(dev)
+    return torch.cuda.get_device_name(dev) if dev.type == "cuda" else dev.type
+
+
+def tune_spmm(H, b, prec=32, reps=3, candidates=CANDIDATES, timer=cuda_event_ms):
+    """Pick and apply the fastest configuration for (H, b, prec); returns (cfg, ms
+    table).  timer(fn, reps) -> ms measures one candidate."""
+    key = (H.n_atoms, H.nnz_blocks, _width_class(b), prec, _device_name(H.device))
     if key in _cache:
         _apply(H, _cache[key][0])
         return _cache[key]
@@ -45,15 +64,15 @@ def tune_spmm(H, b, prec=32, reps=3, candidates=CANDIDATES):
         if cfg[0] == "tiles" and H.tiles is None:
             continue
         _apply(H, cfg)
-        H.matmul(X, out=Y, prec=prec)
-        ev = [(torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)) for _ in range(reps)]
-        for e0, e1 in ev:
-            e0.record()
-            H.matmul(X, out=Y, prec=prec)
-            e1.record()
-        torch.cuda.synchronize()
-        table[cfg] = min(e0.elapsed_time(e1) for e0, e1 in ev)
+        table[cfg] = timer(lambda: H.matmul(X, out=Y, prec=prec), reps)
     best = min(table, key=table.get)
     _apply(H, best)
     _cache[key] = (best, table)
     return best, table
+
+
+def reset():
+    """Forget the cached choices and restore the default launch shape (256 x 5,
+    pair layout kernel)."""
+    _cache.clear()
+    _native.spmm_tune(256, 5)
