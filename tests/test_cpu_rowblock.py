@@ -1,6 +1,7 @@
 """Row-block solver of one structure over several ranks, on CPU: the partition and
 halo plan on real neighbour lists, and the distributed block solver on gloo
-ranks (world sizes 1 and 3, so that a middle rank exchanges halos on both sides)
+ranks (world sizes 1 and 3, so that a middle rank exchanges halos on both sides,
+and 4 on a chain of globules whose ranks exchange with adjacent ranks only)
 with dense row blocks of the oracle Hessian standing in for the GPU store rows.
 Eigenvalues are checked against dense LAPACK, the gathered eigenvectors by their
 residual and orthonormality."""
@@ -16,10 +17,21 @@ from oracle import graph as og
 from oracle import hessian as oh
 
 
-def _structure(n_atoms=400, seed=5):
-    """Atoms in reversed Cuthill-McKee order, their lists, and H + PlusI*I (dense)."""
+def _structure(kind="globule"):
+    """Atoms in reversed Cuthill-McKee order, their lists, and H + PlusI*I (dense).
+    "globule": 400 atoms, a band nearly as wide as the structure; "chain": six
+    touching 250-atom globules along x, whose band is narrow enough that each
+    rank of four exchanges halos with its adjacent ranks only."""
     from inching_b200 import synth
-    X = synth.globule(n_atoms, seed=seed) / 10.0
+    if kind == "globule":
+        X = synth.globule(400, seed=5) / 10.0
+    else:
+        step = 2.0 * synth.globule_radius(250) * 0.95
+        parts = []
+        for i in range(6):
+            g = synth.globule(250, seed=40 + i)
+            parts.append(g - g.mean(axis=0) + np.array([i * step, 0.0, 0.0]))
+        X = np.concatenate(parts) / 10.0
     deg, rp, cl = og.neighbor_lists(X, 8.0)
     order, _ = og.cuthill_mckee(rp, cl, deg)
     Xr = X[order]
@@ -92,7 +104,7 @@ def _free_port():
     return p
 
 
-def _solve(world_rank, world, port, q):
+def _solve(world_rank, world, port, q, kind="globule"):
     import torch.distributed as dist
     from inching_b200.rowblock import (RowBlockComm, RowBlockOperator, chfsi_rowblock, gather_rows, halo_ranges,
                                        row_partition)
@@ -101,7 +113,7 @@ def _solve(world_rank, world, port, q):
         os.environ["MASTER_PORT"] = str(port)
         dist.init_process_group("gloo", rank=world_rank, world_size=world)
     torch.set_num_threads(1)
-    Xr, rp, cl, H = _structure()
+    Xr, rp, cl, H = _structure(kind)
     comm = RowBlockComm()
     parts = row_partition(rp, comm.world)
     ranges = halo_ranges(rp, cl, parts)
@@ -120,8 +132,8 @@ def _solve(world_rank, world, port, q):
     q.put((comm.rank, out))
 
 
-def _check(results):
-    _, _, _, H = _structure()
+def _check(results, kind="globule"):
+    _, _, _, H = _structure(kind)
     w = np.linalg.eigvalsh(H)
     for precision, tol in (("f64", 1e-9), ("mixed", 1e-6)):
         evs = [r[precision][0] for r in results]
@@ -163,3 +175,25 @@ def test_rowblock_solver_gloo_world3():
         assert p.exitcode == 0
     assert got[1]["f64"][1] is None and got[2]["f64"][1] is None    # gathered on rank 0 only
     _check([got[0], got[1], got[2]])
+
+
+def test_rowblock_solver_gloo_world4_chain():
+    from inching_b200.rowblock import exchange_plan, halo_ranges, row_partition
+    _, rp, cl, _ = _structure("chain")
+    parts = row_partition(rp, 4)
+    ranges = halo_ranges(rp, cl, parts)
+    for r in range(4):
+        sends, recvs = exchange_plan(parts, ranges, r)
+        assert {p for p, _, _ in sends} | {p for p, _, _ in recvs} <= {r - 1, r + 1}
+        assert recvs and 0 < ranges[r][1] - ranges[r][0] < len(rp) - 1     # partial halos
+    ctx = mp.get_context("spawn")
+    q = ctx.Queue()
+    port = _free_port()
+    procs = [ctx.Process(target=_solve, args=(r, 4, port, q, "chain")) for r in range(4)]
+    for p in procs:
+        p.start()
+    got = dict(q.get(timeout=300) for _ in procs)
+    for p in procs:
+        p.join(timeout=60)
+        assert p.exitcode == 0
+    _check([got[r] for r in range(4)], "chain")
