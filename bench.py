@@ -312,7 +312,11 @@ def run_ours(args):
                      # ncu dram__bytes_read.sum + dram__bytes_write.sum of one 64-column FP32 launch on this
                      # workload (profiles/spmm_f32_b64_assembly100k.md): 311.8 MB against 318.6 MB algorithmic
                      "traffic": TRAFFIC_B64_BYTES, "traffic_unit": "bytes per 64-column launch",
-                     "traffic_over_algorithmic": TRAFFIC_B64_RATIO},
+                     "traffic_over_algorithmic": TRAFFIC_B64_RATIO,
+                     # what bounds the kernel instead of HBM, from the ncu memory capture of the same
+                     # launch (profiles/spmm_f32_b64_assembly100k_memory.md); not measured by this run
+                     "limiter": {"unit": "L1/TEX data pipe (X_j gathers)", "throughput_frac": 0.793,
+                                 "source": "ncu capture, 64-column FP32 launch on this workload"}},
         "cpu_baseline": cpu,
         "clocks": clk.summary(),
         "gpu_launches": int(launches),
