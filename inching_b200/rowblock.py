@@ -61,15 +61,16 @@ def row_partition(rowptr, world):
 
 def halo_ranges(rowptr, cols, parts):
     """[(lo, hi)] per range: the smallest atom range holding [a, b) and every
-    column of rows a..b-1."""
+    column of rows a..b-1.  The column minima and maxima are taken where cols
+    lives (a device tensor stays on the device)."""
     rp = np.asarray(rowptr.cpu() if torch.is_tensor(rowptr) else rowptr, dtype=np.int64)
-    cl = np.asarray(cols.cpu() if torch.is_tensor(cols) else cols, dtype=np.int64)
     out = []
     for a, b in parts:
-        seg = cl[rp[a]:rp[b]]
-        lo = min(a, int(seg.min())) if seg.size else a
-        hi = max(b, int(seg.max()) + 1) if seg.size else b
-        out.append((lo, hi))
+        seg = cols[int(rp[a]):int(rp[b])]
+        if len(seg):
+            out.append((min(a, int(seg.min())), max(b, int(seg.max()) + 1)))
+        else:
+            out.append((a, b))
     return out
 
 
