@@ -175,3 +175,22 @@ def test_lean_block_solver_chunked_paths_on_dense_double(dense, precision, tol):
     assert np.abs(S.numpy() - w[6:26]).max() < (1e-8 if precision == "f64" else 1e-4) * w[-1]
     assert (V.t() @ V - torch.eye(k, dtype=V.dtype)).abs().max() < 1e-10
     assert (dense["Q"] @ V).abs().max() < 1e-10
+
+
+@pytest.mark.parametrize("name,k,tol", [("trlm", 12, 1e-10), ("jdm", 12, 1e-8), ("irlm", 32, 1e-10)])
+def test_reference_solver_control_flow_on_dense_double(dense, name, k, tol):
+    """The reference algorithms' host control flow (TRLM thick restarts, JDM with
+    its projected GMRES correction and locking, IRLM implicit restarts) with
+    Hotelling deflation of the rigid modes, on the dense test double: the
+    eigenvalues of dense LAPACK and orthonormal eigenvectors orthogonal to the
+    rigid-body basis.  IRLM keeps the reference's refusal of fewer than 32 modes."""
+    import importlib
+    fn = getattr(importlib.import_module(f"inching_b200.solvers.{name}"), name)
+    w = dense["w"]
+    S, V = fn(dense["F"], k=k, tol=tol, Q=dense["Q"], shift=10.0)[:2]
+    assert np.abs(S.numpy() - w[6:6 + k]).max() < 1e-10 * w[-1]
+    assert (V.t() @ V - torch.eye(k, dtype=V.dtype)).abs().max() < 1e-8
+    assert (dense["Q"] @ V).abs().max() < 1e-8
+    if name == "irlm":
+        with pytest.raises(AssertionError, match="ABORTED"):
+            fn(dense["F"], k=16, tol=tol, Q=dense["Q"], shift=10.0)
