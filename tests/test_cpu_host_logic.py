@@ -194,3 +194,25 @@ def test_reference_solver_control_flow_on_dense_double(dense, name, k, tol):
     if name == "irlm":
         with pytest.raises(AssertionError, match="ABORTED"):
             fn(dense["F"], k=16, tol=tol, Q=dense["Q"], shift=10.0)
+
+
+def test_ctrlm_march_and_resume_on_dense_double(dense, tmp_path):
+    """Interval marching on the dense double: one window written to the
+    reference's window pickles, then a second call resumes from them.  Together
+    the two calls find the 40 lowest non-rigid modes of dense LAPACK with no
+    duplicate and no gap, and each window has its Eigval / PerformanceList file."""
+    from inching_b200.ctrlm import ctrlm_many_modes
+    F = dense["F"]
+    F.plus_i, F.n_atoms = 1.0, F.shape[0] // 3
+    w = dense["w"] - 1.0
+    ck = dict(folder=str(tmp_path), pdbid="toy", platform="Linux", device="cpu")
+    a = ctrlm_many_modes(F, 40, n_mode=16, Q=dense["Q"], tol=1e-10, checkpoint=ck, max_windows=1)
+    assert not a["complete"] and len(a["windows"]) == 1
+    b = ctrlm_many_modes(F, 40, n_mode=16, Q=dense["Q"], tol=1e-10, checkpoint=ck)
+    assert b["complete"] and b["windows"][0]["offset"] == len(a["eigvals"])
+    ev = np.sort(np.concatenate([a["eigvals"], b["eigvals"]]))
+    assert len(ev) >= 40 and np.diff(ev).min() > 1e-6
+    assert np.abs(ev[:40] - w[6:46]).max() < 1e-10 * w[-1]
+    for win in a["windows"] + b["windows"]:
+        for kind in ("Eigval", "PerformanceList"):
+            assert (tmp_path / f"{kind}_InchingManyCTRLM_toy_Linux_cpu_{win['offset']}.pkl").exists()
