@@ -216,3 +216,28 @@ def test_ctrlm_march_and_resume_on_dense_double(dense, tmp_path):
     for win in a["windows"] + b["windows"]:
         for kind in ("Eigval", "PerformanceList"):
             assert (tmp_path / f"{kind}_InchingManyCTRLM_toy_Linux_cpu_{win['offset']}.pkl").exists()
+
+
+def test_solver_facades_on_dense_double(dense):
+    """The drop-in solver entry points with the reference's argument names
+    (A, A_diag, k, tol, User_Q_HotellingDeflation, ...) return its layout:
+    eigenvalues including PlusI and eigenvectors as (n, k) columns; and they
+    keep the reference's refusals (JDM with a polynomial filter or a workspace
+    factor <= 1, TRLM with k >= n)."""
+    from inching_b200.Burn.ImplicitlyRestartedLanczosHotellingDeflation.T1 import S_HeigvalIRLMHD_HeigvecIRLMHD
+    from inching_b200.Burn.JacobiDavidsonHotellingDeflation.T1 import S_HeigvalJDMHD_HeigvecJDMHD
+    from inching_b200.Burn.ThickRestartLanczosHotellingDeflation.T1 import S_HeigvalTRLMHD_HeigvecTRLMHD
+    F, Q, w = dense["F"], dense["Q"], dense["w"]
+    Ad = torch.from_numpy(np.diag(F.Hd.numpy()).copy())
+    n = F.shape[0]
+    for S, V, k in ((*S_HeigvalTRLMHD_HeigvecTRLMHD(F, Ad, k=12, tol=1e-10, User_Q_HotellingDeflation=Q)[:2], 12),
+                    (*S_HeigvalJDMHD_HeigvecJDMHD(F, Ad, k=12, tol=1e-8, User_Q_HotellingDeflation=Q)[:2], 12),
+                    (*S_HeigvalIRLMHD_HeigvecIRLMHD(F, k=32, tol=1e-10, User_Q_HotellingDeflation=Q)[:2], 32)):
+        assert tuple(V.shape) == (n, k)
+        assert np.abs(np.sort(np.asarray(S.cpu())) - w[6:6 + k]).max() < 1e-10 * w[-1]
+    with pytest.raises(AssertionError, match="ABORTED"):
+        S_HeigvalJDMHD_HeigvecJDMHD(F, Ad, k=12, User_WorkspaceSizeFactor=1)
+    with pytest.raises(AssertionError, match="ABORTED"):
+        S_HeigvalJDMHD_HeigvecJDMHD(F, Ad, k=12, User_PolynomialParams=object())
+    with pytest.raises(AssertionError, match="ABORTED"):
+        S_HeigvalTRLMHD_HeigvecTRLMHD(F, Ad, k=n)
