@@ -241,3 +241,39 @@ def test_solver_facades_on_dense_double(dense):
         S_HeigvalJDMHD_HeigvecJDMHD(F, Ad, k=12, User_PolynomialParams=object())
     with pytest.raises(AssertionError, match="ABORTED"):
         S_HeigvalTRLMHD_HeigvecTRLMHD(F, Ad, k=n)
+
+
+def test_operator_facades_against_oracle_on_dense_double(dense):
+    """Krylov aux(A, v, u), the Hotelling update, ChebyshevAv (with the KPM rho)
+    and the Lanczos spectrum bound through the drop-in module paths, against the
+    oracle's restatements of Krylov/T3.py, Orthogonalization/T3.py and
+    PolynomialFilters/T2.py on the dense test double."""
+    from oracle import solvers as osv
+    from inching_b200 import polyfilter
+    from inching_b200.Burn.HermitianLanczos.T2 import A_Adiag_EstimateSpectrumBound
+    from inching_b200.Burn.Krylov.T3 import OOC2_FullMemS_v_KrylovAv_VOID, OOC2_HalfMemS_v_KrylovAv_VOID
+    from inching_b200.Burn.Orthogonalization.T3 import T3_QHotelling_x_Ax_HotelledAx
+    from inching_b200.Burn.PolynomialFilters.T2 import OOC2_A_Adiag_ChebyshevAv
+    F, Q, w = dense["F"], dense["Q"], dense["w"]
+    Hd = F.Hd.numpy()
+    Ad = torch.from_numpy(np.diag(Hd).copy())
+    v = torch.from_numpy(np.random.default_rng(2).standard_normal(F.shape[0]))
+    for factory in (OOC2_HalfMemS_v_KrylovAv_VOID, OOC2_FullMemS_v_KrylovAv_VOID):
+        u = torch.empty_like(v)
+        assert factory(F, Ad)(F, v, u) is None
+        assert np.abs(u.numpy() - Hd @ v.numpy()).max() < 1e-12 * np.abs(Hd).max()
+    res = torch.zeros_like(v)
+    T3_QHotelling_x_Ax_HotelledAx(Q, v, res, HotellingShift=-40.0)
+    ref = oh.hotelling(Q.numpy(), v.numpy(), np.zeros(F.shape[0]), -40.0)
+    assert np.abs(res.numpy() - ref).max() < 1e-12 * np.abs(ref).max()
+    lo, hi = A_Adiag_EstimateSpectrumBound(F, Ad)
+    assert abs(hi - w[-1]) < 1e-6 * w[-1] and abs(lo - w[0]) < 1e-6 * w[-1]
+    pol = polyfilter.OOC0_OptimizePolynomialParamsOnDegree(User_WantedInterval=(1.0, 3.0),
+                                                           User_SpectrumBound=(0.99, w[-1] * 1.01),
+                                                           User_MaximumDegree=300)
+    ref = osv.chebyshev_av(lambda x: Hd @ x, v.numpy(), pol.AdjustedCoefficients, pol.cc, pol.dd, pol.AdjustedDegree)
+    for precision, tol in (("f64", 1e-10), ("mixed", 1e-4)):
+        y = OOC2_A_Adiag_ChebyshevAv(F, Ad, User_PolynomialParams=pol, User_Precision=precision).ChebyshevAv(F, v)
+        assert np.abs(y.double().numpy() - ref).max() <= tol * np.abs(ref).max()
+    with pytest.raises(AssertionError, match="ABORTED"):
+        OOC2_A_Adiag_ChebyshevAv(F, Ad)
