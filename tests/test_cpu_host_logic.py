@@ -277,3 +277,29 @@ def test_operator_facades_against_oracle_on_dense_double(dense):
         assert np.abs(y.double().numpy() - ref).max() <= tol * np.abs(ref).max()
     with pytest.raises(AssertionError, match="ABORTED"):
         OOC2_A_Adiag_ChebyshevAv(F, Ad)
+
+
+def test_cdm_and_kpm_facades_on_dense_double(dense):
+    """Chebyshev-Davidson through the reference signature (no deflation: the six
+    rigid modes at PlusI come first) against dense LAPACK, its three refusals, and
+    the KPM eigenvalue count of a window within 30 % of the true count."""
+    from inching_b200 import polyfilter
+    from inching_b200.Burn.ChebyshevDavidsonSubspaceIteration.T1 import (OOC2_KrylovAv_A_EstimateSpectrumBound,
+                                                                           S_HeigvalCDSIHD_HeigvecCDSIHD)
+    from inching_b200.Burn.PolynomialFilters.T2 import A_Adiag_PolynomialParams_KpmEstimate
+    F, Q, w = dense["F"], dense["Q"], dense["w"]
+    Ad = torch.from_numpy(np.diag(F.Hd.numpy()).copy())
+    bound = OOC2_KrylovAv_A_EstimateSpectrumBound(None, F)
+    S, V = S_HeigvalCDSIHD_HeigvecCDSIHD(F, Ad, k=16, tol=1e-10, User_ChebyshevDegree=20, User_SpectrumBound=bound)
+    assert np.max(np.abs(np.asarray(S.cpu()) - w[:16]) / w[:16]) < 1e-9
+    for bad in (dict(User_SpectrumBound=None), dict(User_SpectrumBound=bound, User_WorkspaceSizeFactor=1),
+                dict(User_SpectrumBound=bound, User_Q_HotellingDeflation=Q)):
+        with pytest.raises(AssertionError, match="ABORTED"):
+            S_HeigvalCDSIHD_HeigvecCDSIHD(F, Ad, k=16, **bad)
+    lo, hi = 0.5 * (w[9] + w[10]), 0.5 * (w[80] + w[81])
+    pol = polyfilter.OOC0_OptimizePolynomialParamsOnDegree(User_WantedInterval=(lo, hi),
+                                                           User_SpectrumBound=(w[0] - 1e-3, w[-1] * 1.01),
+                                                           User_MaximumDegree=3000)
+    true = int(np.sum((w >= lo) & (w <= hi)))
+    est = A_Adiag_PolynomialParams_KpmEstimate(F, Ad, User_PolynomialParams=pol, User_NumberKpmTrials=400)
+    assert abs(est - true) <= 0.3 * true
