@@ -303,3 +303,56 @@ def test_cdm_and_kpm_facades_on_dense_double(dense):
     true = int(np.sum((w >= lo) & (w <= hi)))
     est = A_Adiag_PolynomialParams_KpmEstimate(F, Ad, User_PolynomialParams=pol, User_NumberKpmTrials=400)
     assert abs(est - true) <= 0.3 * true
+
+
+class RankOneStore:
+    """Host view of the rank-one store built by the oracle: cutoff lists and FP64
+    entries {wx, wy, wz, col} with w = (x_j - x_i) / |x_j - x_i| (0 for the self
+    entry), as the Galerkin bead operator reads them."""
+
+    def __init__(self, X):
+        from oracle import graph as og
+        deg, rp, cl = og.neighbor_lists(X, 8.0)
+        n = X.shape[0]
+        rows = np.repeat(np.arange(n), np.diff(rp))
+        d = X[cl] - X[rows]
+        nrm = np.linalg.norm(d, axis=1)
+        w = np.where(nrm[:, None] > 0, d / np.where(nrm > 0, nrm, 1.0)[:, None], 0.0)
+        self.X = torch.from_numpy(X)
+        self.rowptr = torch.from_numpy(np.asarray(rp, np.int64))
+        self.cols = torch.from_numpy(np.asarray(cl, np.int32))
+        self.ent64 = torch.from_numpy(np.c_[w, cl.astype(np.float64)])
+        self.ent32 = None
+        self.n_atoms, self.plus_i, self.device = n, 1.0, torch.device("cpu")
+        self.shape = (3 * n, 3 * n)
+
+
+def test_galerkin_bead_operator_and_start_on_cpu():
+    """The Galerkin bead operator built from the store's w entries equals
+    M^-1/2 P^T H P M^-1/2 of the oracle Hessian, and the Galerkin start's block
+    V = P M^-1/2 Z is orthonormal with V^T H V carrying the operator's lowest
+    non-rigid eigenvalues."""
+    import scipy.sparse as sp
+    from inching_b200 import synth
+    from inching_b200.warmstart import GalerkinOperator, bead_model, galerkin_warm_start
+    X = synth.globule(600, seed=8) / 10.0
+    H = RankOneStore(X)
+    A, Ad = oh.hessian_lower(X, 8.0, 1.0)
+    Hd = oh.full_from_lower(A, Ad).toarray()
+    _, bead = bead_model(H.X, 6.0)
+    nb = int(bead.max()) + 1
+    counts = torch.bincount(bead, minlength=nb)
+    G = GalerkinOperator(H, bead, nb, counts)
+    n = H.n_atoms
+    bd = bead.numpy()
+    P = sp.csr_matrix((np.ones(3 * n), (np.arange(3 * n), 3 * np.repeat(bd, 3) + np.tile([0, 1, 2], n))),
+                      shape=(3 * n, 3 * nb))
+    Mh = 1.0 / np.sqrt(np.repeat(counts.numpy(), 3).astype(float))
+    S = (sp.diags(Mh) @ (P.T @ sp.csr_matrix(Hd) @ P) @ sp.diags(Mh)).toarray()
+    assert np.abs(G.csr64.to_dense().numpy() - S).max() < 1e-12 * np.abs(S).max()
+    V, info = galerkin_warm_start(H, 24, tol=1e-6, return_info=True)
+    assert V.shape == (3 * n, 24) and info["beads"] == nb
+    assert (V.t() @ V - torch.eye(24, dtype=V.dtype)).abs().max() < 1e-10
+    theta = np.linalg.eigvalsh((V.t() @ torch.from_numpy(Hd) @ V).numpy())
+    sigma = np.linalg.eigvalsh(S)[6:30]
+    assert np.abs(theta - sigma).max() < 1e-6 * sigma[-1]
