@@ -62,6 +62,8 @@ def parse():
                     "solver's size rule)")
     ap.add_argument("--profile", action="store_true", help="cube2400k: CUDA-event phase times of the solver")
     ap.add_argument("--layout", default="tiles", choices=["tiles", "pairs"], help="store layout for --kernel-only")
+    ap.add_argument("--band-panel", type=int, default=None, choices=[64, 128],
+                    help="widest FP32 panel of the band-tile product (--kernel-only)")
     return ap.parse_args()
 
 
@@ -76,6 +78,8 @@ def run_kernel_only(args):
     if args.tune:
         t, bps = (int(x) for x in args.tune.split(","))
         _native.spmm_tune(t, bps)
+    if args.band_panel:
+        _native.spmm_band_tune(args.band_panel)
     Xd = torch.from_numpy(synth.workload(args.workload) / 10.0).cuda()
     order, _ = graph.cuthill_mckee(Xd, 8.0)
     prec = 32 if args.kernel_only == "spmm32" else 64
@@ -95,7 +99,8 @@ def run_kernel_only(args):
     ms = [e0.elapsed_time(e1) for e0, e1 in ev]
     nbytes = H.store_bytes(prec, args.b) + 2 * X.numel() * X.element_size()
     best = min(ms)
-    print(json.dumps({"kernel": args.kernel_only, "b": args.b, "tune": args.tune, "layout": args.layout, "n_atoms": H.n_atoms, "nnz": H.nnz_blocks,
+    print(json.dumps({"kernel": args.kernel_only, "b": args.b, "tune": args.tune, "layout": args.layout,
+                      "band_panel": args.band_panel, "n_atoms": H.n_atoms, "nnz": H.nnz_blocks,
                       "ms": [round(m, 4) for m in ms], "algorithmic_bytes": nbytes,
                       "best_GBps": round(nbytes / best / 1e6, 1)}))
 

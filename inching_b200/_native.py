@@ -108,6 +108,10 @@ _SIGS = {
     "inch_spmm_tiles": (ctypes.c_int, [c_int32, c_int64, c_void_p, c_void_p, c_void_p, c_void_p, c_void_p,
                                        c_void_p, c_int64, c_int32, c_void_p, c_int64, c_void_p, c_int64, c_void_p,
                                        c_int64, c_void_p, POINTER(SpmmEpilogue), c_void_p, c_size_t, c_void_p]),
+    "inch_spmm_tiles_seg": (ctypes.c_int, [c_int32, c_int64, c_void_p, c_void_p, c_void_p, c_void_p, c_void_p,
+                                           c_void_p, c_int64, c_int32, c_void_p, c_int64, c_void_p, c_int64,
+                                           c_void_p, c_void_p, c_void_p]),
+    "inch_spmm_band_tune": (ctypes.c_int, [c_int32]),
     "inch_hessian_assemble_weighted": (ctypes.c_int, [c_void_p, c_int64, c_double, c_double, c_void_p, c_void_p,
                                                       c_void_p, c_void_p, c_void_p, c_void_p, c_void_p, c_void_p]),
     "inch_mp_edge_concat": (ctypes.c_int, [c_void_p, c_void_p, c_void_p, c_int64, c_int32, c_int32, c_void_p,
@@ -276,6 +280,8 @@ def hessian_assemble(X, rowptr, cols, rc_nm, plus_i, want64=True, want32=True, p
     if image is not None:
         assert pair_weight is None, "ABORTED. periodic images and pair weights are not combined"
         _require_cuda(image, "image", torch.int8)
+        if image.numel() != nnz:
+            raise AssertionError(f"ABORTED. image holds {image.numel()} codes for {nnz} adjacency entries")
         check(lib().inch_hessian_assemble_pbc_xy(_ptr(X), n, rc_nm, plus_i, _ptr(rowptr), _ptr(cols), _ptr(image),
                                                  float(box_xy[0]), float(box_xy[1]), _ptr(ent64), _ptr(diag64),
                                                  _ptr(ent32), _ptr(diag32), _stream()))
@@ -284,6 +290,11 @@ def hessian_assemble(X, rowptr, cols, rc_nm, plus_i, want64=True, want32=True, p
                                           _ptr(diag64), _ptr(ent32), _ptr(diag32), _stream()))
     else:
         _require_cuda(pair_weight, "pair_weight", torch.float64)
+        if pair_weight.numel() != nnz:
+            raise AssertionError(f"ABORTED. pair_weight holds {pair_weight.numel()} springs for {nnz} adjacency "
+                                 "entries")
+        if bool((pair_weight < 0).any()):
+            raise AssertionError("ABORTED. pair_weight must be non-negative (each block is -gamma u u^T)")
         check(lib().inch_hessian_assemble_weighted(_ptr(X), n, rc_nm, plus_i, _ptr(rowptr), _ptr(cols),
                                                    _ptr(pair_weight), _ptr(ent64), _ptr(diag64), _ptr(ent32),
                                                    _ptr(diag32), _stream()))
@@ -397,13 +408,42 @@ def spmm_tiles(prec, n_atoms, uptr, pptr, urec, pw, diag, X, Y, *, alpha=1.0, ga
     check(L.inch_spmm_tiles(prec, n_atoms, _ptr(uptr), _ptr(pptr), _ptr(urec), _ptr(pw), _ptr(diag), _ptr(X), ldx,
                             b, _ptr(Y), ldy, _ptr(Yin), ldyin, _ptr(acc), ldacc, _ptr(Q), ctypes.byref(ep),
                             _ptr(ws), ws.numel(), _stream()))
-    tiles = 0
+    _count(band_panels(prec, b) * (3 if r > 0 else 1))
+    return Y
+
+
+_band_widest32 = 128
+
+
+def band_panels(prec, b):
+    """Kernel launches of one band-tile product of b columns: panels of 128 (FP32,
+    when selected), 64 and 32 columns, the last one partial."""
+    n = 0
     rem = b
-    for t in ((64, 32, 16, 8, 4, 2, 1) if prec == 32 else (32, 16, 8, 4, 2, 1)):
-        while rem >= t:
-            rem -= t
-            tiles += 1
-    _count(tiles * (3 if r > 0 else 1))
+    for w in (((_band_widest32, 64) if _band_widest32 == 128 else (64,)) if prec == 32 else (64,)):
+        while rem >= w:
+            rem -= w
+            n += 1
+    return n + (rem + 31) // 32
+
+
+def spmm_band_tune(widest_fp32_panel=128):
+    """Widest FP32 panel of the band-tile product for this process: 128 or 64."""
+    global _band_widest32
+    check(lib().inch_spmm_band_tune(widest_fp32_panel))
+    _band_widest32 = int(widest_fp32_panel)
+
+
+def spmm_tiles_seg(prec, n_atoms, uptr, pptr, urec, pw, diag, X, Y, atom_seg, seg_coef, Yin=None):
+    """spmm_seg() on the row-tile store (any number of columns)."""
+    L = lib()
+    b = 1 if X.dim() == 1 else X.shape[1]
+    ldx = 1 if X.dim() == 1 else X.stride(0)
+    ldy = 1 if Y.dim() == 1 else Y.stride(0)
+    ldyin = 0 if Yin is None else (1 if Yin.dim() == 1 else Yin.stride(0))
+    check(L.inch_spmm_tiles_seg(prec, n_atoms, _ptr(uptr), _ptr(pptr), _ptr(urec), _ptr(pw), _ptr(diag), _ptr(X),
+                                ldx, b, _ptr(Y), ldy, _ptr(Yin), ldyin, _ptr(atom_seg), _ptr(seg_coef), _stream()))
+    _count(band_panels(prec, b))
     return Y
 
 

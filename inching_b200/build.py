@@ -15,7 +15,22 @@ import sys
 HERE = os.path.dirname(os.path.abspath(__file__))
 CSRC = os.path.join(HERE, "csrc")
 LIB = os.path.join(HERE, "libinching_b200.so")
-NVCC = os.environ.get("NVCC", "/usr/local/cuda/bin/nvcc")
+
+
+def _cuda_home() -> str:
+    """Toolkit root: $CUDA_HOME / $CUDA_PATH, else the directory above the nvcc on PATH."""
+    for var in ("CUDA_HOME", "CUDA_PATH"):
+        if os.environ.get(var):
+            return os.environ[var]
+    import shutil
+    nv = shutil.which("nvcc")
+    if nv:
+        return os.path.dirname(os.path.dirname(os.path.realpath(nv)))
+    raise RuntimeError("no CUDA toolkit: set CUDA_HOME or put nvcc on PATH")
+
+
+CUDA_HOME = _cuda_home()
+NVCC = os.environ.get("NVCC", os.path.join(CUDA_HOME, "bin", "nvcc"))
 
 NVCC_FLAGS = [
     "-O3", "-std=c++17", "-lineinfo",
@@ -67,7 +82,7 @@ def build(force: bool = False, verbose: bool = False) -> str:
     # cuBLAS for the tall-skinny GEMMs of the block-solver entry points; the rpath
     # finds the toolkit's copy when no other libcublas.so.12 is loaded already
     cmd = [NVCC, "-shared", "-gencode", "arch=compute_100a,code=sm_100a", *objs, "-lcublas",
-           "-Xlinker", "-rpath=/usr/local/cuda/lib64", "-o", tmp]
+           "-Xlinker", "-rpath=" + os.path.join(CUDA_HOME, "lib64"), "-o", tmp]
     r = subprocess.run(cmd, stdout=subprocess.PIPE, stderr=subprocess.STDOUT)
     if r.returncode != 0:
         raise RuntimeError("link failed:\n" + r.stdout.decode())

@@ -397,20 +397,27 @@ k_qx_partial(const double* __restrict__ Q, int64_t ndof, const T* __restrict__ X
   __shared__ double s[kThreads];
   s[threadIdx.x] = acc;
   __syncthreads();
-  if (threadIdx.x < B) {
-    double t = 0.0;
-    for (int u = threadIdx.x; u < kThreads; u += B) t += s[u];
-    partial[((int64_t)blockIdx.x * r + q) * B + threadIdx.x] = t;
+  // tree over the threads of one column (B is a power of two dividing kThreads,
+  // so t and t + stride always share a column): log2(kThreads / B) steps
+#pragma unroll
+  for (int stride = kThreads / 2; stride >= B; stride >>= 1) {
+    if (threadIdx.x < stride) s[threadIdx.x] += s[threadIdx.x + stride];
+    __syncthreads();
   }
+  if (threadIdx.x < B) partial[((int64_t)blockIdx.x * r + q) * B + threadIdx.x] = s[threadIdx.x];
 }
 
-__global__ void k_qx_final(const double* __restrict__ partial, int P, int r, int B, double shift,
-                           double* __restrict__ coef) {
-  for (int t = threadIdx.x; t < r * B; t += blockDim.x) {
-    double s = 0.0;
-    for (int p = 0; p < P; ++p) s += partial[(int64_t)p * r * B + t];
-    coef[t] = shift * s;
-  }
+// coef[t] = shift * sum_p partial[p, t]: one warp per output (vector, column), its
+// lanes striding over the P partials, then a fixed shuffle tree (deterministic).
+__global__ void __launch_bounds__(kThreads)
+k_qx_final(const double* __restrict__ partial, int P, int r, int B, double shift, double* __restrict__ coef) {
+  const int t = blockIdx.x * (kThreads / 32) + (threadIdx.x >> 5);
+  if (t >= r * B) return;
+  const int lane = threadIdx.x & 31;
+  double s = 0.0;
+  for (int p = lane; p < P; p += 32) s += partial[(int64_t)p * r * B + t];
+  s = warp_sum(s);
+  if (lane == 0) coef[t] = shift * s;
 }
 
 constexpr int kQxBlocks = 296;
@@ -424,7 +431,8 @@ cudaError_t launch_tile(int64_t n_atoms, const int64_t* rowptr, const void* ent,
   if (ep.r > 0) {
     dim3 g(kQxBlocks, ep.r);
     k_qx_partial<T, B><<<g, kThreads, 0, stream>>>(Q, ndof, X, ldx, c0, partial);
-    k_qx_final<<<1, 512, 0, stream>>>(partial, kQxBlocks, ep.r, B, hot_shift, coef);
+    k_qx_final<<<(ep.r * B + kThreads / 32 - 1) / (kThreads / 32), kThreads, 0, stream>>>(partial, kQxBlocks,
+                                                                                          ep.r, B, hot_shift, coef);
   }
   if constexpr (G == 0) {
     // Vector (V = 2) gathers need X, Y (and Yin / Acc when used) rows aligned to
@@ -587,8 +595,9 @@ extern "C" inch_status inch_spmm(int32_t prec, int64_t n_atoms, const int64_t* r
 // 1.2 MB, resident on every GPU that loads the library until the process exits.
 // The array's host-side name is not a device address: its address is fetched
 // with cudaGetSymbolAddress once per device, with that device current, on the
-// first call made on that device (so make that first call before any stream
-// capture).  Nothing in the array has to start at zero: every call writes each
+// first call with deflation vectors (r > 0) made on that device, so make that
+// first call before any stream capture; calls with r = 0 never touch the array.
+// Nothing in the array has to start at zero: every call writes each
 // partial sum and coefficient before reading it.  All calls share the array, so
 // calls that overlap on the GPU (different streams, or different host threads on
 // the same device) race on it and must be serialised by the caller.
@@ -628,21 +637,27 @@ extern "C" inch_status inch_spmm_noalloc(int32_t prec, int64_t n_atoms, const in
                "inch_spmm_noalloc: accumulate needs Acc");
   INCH_REQUIRE(((uintptr_t)ent & 15) == 0 && ((uintptr_t)diag & 15) == 0, INCH_INVALID_ARG,
                "inch_spmm_noalloc: store buffers must be 16-byte aligned");
-  int dev = -1;
-  INCH_CUDA(cudaGetDevice(&dev));
-  INCH_REQUIRE(dev >= 0 && dev < kNoAllocMaxDevices, INCH_LIMIT, "inch_spmm_noalloc: device %d not supported", dev);
-  double* base = nullptr;
-  {
-    std::lock_guard<std::mutex> lock(g_noalloc_mu);
-    if (g_noalloc_addr[dev] == nullptr) {
-      void* p = nullptr;
-      INCH_CUDA(cudaGetSymbolAddress(&p, g_noalloc_scratch));
-      g_noalloc_addr[dev] = static_cast<double*>(p);
+  double *partial = nullptr, *coef = nullptr;
+  if (e.r > 0) {
+    // the static scratch holds only the deflation partial sums: look its device
+    // address up (once per device) only for calls that use it
+    int dev = -1;
+    INCH_CUDA(cudaGetDevice(&dev));
+    INCH_REQUIRE(dev >= 0 && dev < kNoAllocMaxDevices, INCH_LIMIT, "inch_spmm_noalloc: device %d not supported",
+                 dev);
+    double* base = nullptr;
+    {
+      std::lock_guard<std::mutex> lock(g_noalloc_mu);
+      if (g_noalloc_addr[dev] == nullptr) {
+        void* p = nullptr;
+        INCH_CUDA(cudaGetSymbolAddress(&p, g_noalloc_scratch));
+        g_noalloc_addr[dev] = static_cast<double*>(p);
+      }
+      base = g_noalloc_addr[dev];
     }
-    base = g_noalloc_addr[dev];
+    partial = base;
+    coef = base + kNoAllocPartial;
   }
-  double* partial = base;
-  double* coef = base + kNoAllocPartial;
   Epi ep{e.alpha, e.gamma, e.beta, e.mu, e.r, e.accumulate, (e.beta != 0.0) ? 1 : 0};
   cudaError_t err;
   if (prec == 32)

@@ -15,6 +15,8 @@
 // gathered once per distinct column and applied, through the mask, to every row
 // of the tile that needs it (unrolled over the 8 rows, so accumulators stay in
 // registers).  Diagonal blocks and the fused epilogue are those of spmm.cu.
+#include <atomic>
+
 #include <cub/cub.cuh>
 
 #include "common.cuh"
@@ -98,206 +100,511 @@ __global__ void k_set0_pair(int64_t* a, int64_t* b) {
   b[0] = 0;
 }
 
-template <class T>
-struct PW;
-template <>
-struct PW<float> {
-  __device__ __forceinline__ static void load(const void* base, int64_t p, float& wx, float& wy, float& wz) {
-    const float4 v = __ldg(reinterpret_cast<const float4*>(base) + p);
-    wx = v.x;
-    wy = v.y;
-    wz = v.z;
-  }
-};
-template <>
-struct PW<double> {
-  __device__ __forceinline__ static void load(const void* base, int64_t p, double& wx, double& wy, double& wz) {
-    const double2* q = reinterpret_cast<const double2*>(base) + 2 * p;
-    const double2 a = __ldg(q), b = __ldg(q + 1);
-    wx = a.x;
-    wy = a.y;
-    wz = b.x;
-  }
-};
-
-template <class T, int V>
-__device__ __forceinline__ void vld2(const T* p, T (&x)[V]) {
-  if constexpr (V == 1) {
-    x[0] = __ldg(p);
-  } else if constexpr (sizeof(T) == 4) {
-    const float2 v = __ldg(reinterpret_cast<const float2*>(p));
-    x[0] = v.x;
-    x[1] = v.y;
-  } else {
-    const double2 v = __ldg(reinterpret_cast<const double2*>(p));
-    x[0] = v.x;
-    x[1] = v.y;
-  }
-}
+// ---------------------------------------------------------------------------
+// Band-tile product (union walk).
+//
+// One warp owns one 8-row tile and one column panel of P = 32*C columns; lane l
+// owns the C consecutive columns [l*C, l*C + C) of the panel.  The tile's union
+// records arrive 32 at a time (one coalesced load; the next batch is loaded one
+// batch ahead), an exclusive warp scan of popc(mask) gives each union column's
+// first pair, and the batch's w (at most 256 pairs) is staged once in this
+// warp's slice of shared memory, so every pair reads its w as one broadcast
+// shared load.  X_j of union column u is gathered once (three coalesced row
+// segments of P values) two columns ahead of its use (two register sets, A for
+// even and B for odd union columns) and applied to every row of the mask.  The
+// mask is split in two nibbles; each nibble dispatches through a 16-way switch
+// to straight-line code with the accumulator rows fixed at compile time, so the
+// accumulators stay in registers and no per-row bit test is executed.
+//
+// FP32 panels with C >= 2 use the packed f32x2 FMAs of sm_100 (two columns per
+// instruction); the staged w is stored pre-broadcast ({wx,wx,wy,wy},{wz,wz,0,0})
+// so that its halves are the f32x2 operands directly.  The accumulators hold
+// S = sum_j w (w . X_j); the epilogue forms (H X)_i = D_i X_i - S.
+// ---------------------------------------------------------------------------
+constexpr int kUB = 32;                    // union records per batch
+constexpr int kBatchPairs = kUB * kTile;   // pairs of one batch, at most
+constexpr int kWarpsUT = 4;                // warps per block
+constexpr int kMaxPanel = 128;             // widest panel (FP32, C = 4)
 
 struct EpiT {
   double alpha, gamma, beta, mu;
   int r, accumulate, has_yin;
+  const double* seg_coef;   // optional per-segment (alpha, gamma, beta)
+  const int* atom_seg;
 };
 
-constexpr int kThreads = 256;
+template <class T>
+struct Stage;
+template <>
+struct Stage<float> {
+  float4 a, b;   // {wx,wx,wy,wy}, {wz,wz,0,0}
+  __device__ __forceinline__ static void fill(Stage* s, const void* pw, int64_t p) {
+    const float4 v = __ldg(reinterpret_cast<const float4*>(pw) + p);
+    s->a = make_float4(v.x, v.x, v.y, v.y);
+    s->b = make_float4(v.z, v.z, 0.f, 0.f);
+  }
+};
+template <>
+struct Stage<double> {
+  double2 a, b;  // {wx,wy}, {wz,0}
+  __device__ __forceinline__ static void fill(Stage* s, const void* pw, int64_t p) {
+    const double2* q = reinterpret_cast<const double2*>(pw) + 2 * p;
+    s->a = __ldg(q);
+    s->b = __ldg(q + 1);
+  }
+};
 
-// One group of LPR lanes per tile; lane owns V consecutive columns per chunk.
-template <class T, int B, int V>
-__global__ void __launch_bounds__(kThreads)
-k_spmm_tiles(int64_t n_atoms, const int64_t* __restrict__ uptr, const int64_t* __restrict__ pptr,
-             const uint32_t* __restrict__ urec, const void* __restrict__ pw, const T* __restrict__ diag,
-             const T* __restrict__ X, int64_t ldx, T* Y, int64_t ldy, const T* Yin, int64_t ldyin,
-             T* __restrict__ Acc, int64_t ldacc, int c0, EpiT ep, const double* __restrict__ Q, int64_t ndof,
-             const double* __restrict__ coef) {
-  constexpr int LPR = (B / V) < 32 ? (B / V) : 32;
-  constexpr int CPL = B / (LPR * V);
-  constexpr int GPW = 32 / LPR;
-  constexpr int GPB = (kThreads / 32) * GPW;
-  __shared__ double s_coef[8 * B];
+// Register vector type of one lane's columns: NV values of type V.
+template <class T, int C>
+struct UK;
+template <>
+struct UK<float, 4> {
+  using V = float2;
+  static constexpr int NV = 2;
+  static constexpr int MINB = 3;
+};
+template <>
+struct UK<float, 2> {
+  using V = float2;
+  static constexpr int NV = 1;
+  static constexpr int MINB = 4;
+};
+template <>
+struct UK<float, 1> {
+  using V = float;
+  static constexpr int NV = 1;
+  static constexpr int MINB = 4;
+};
+template <>
+struct UK<double, 2> {
+  using V = double;
+  static constexpr int NV = 2;
+  static constexpr int MINB = 3;
+};
+template <>
+struct UK<double, 1> {
+  using V = double;
+  static constexpr int NV = 1;
+  static constexpr int MINB = 4;
+};
+
+__device__ __forceinline__ float2 vmul(float2 a, float2 b) { return __fmul2_rn(a, b); }
+__device__ __forceinline__ float2 vfma(float2 a, float2 b, float2 c) { return __ffma2_rn(a, b, c); }
+__device__ __forceinline__ float vmul(float a, float b) { return a * b; }
+__device__ __forceinline__ float vfma(float a, float b, float c) { return fmaf(a, b, c); }
+__device__ __forceinline__ double vmul(double a, double b) { return a * b; }
+__device__ __forceinline__ double vfma(double a, double b, double c) { return fma(a, b, c); }
+
+__device__ __forceinline__ void get_w(const Stage<float>& s, float2& wx, float2& wy, float2& wz) {
+  wx = make_float2(s.a.x, s.a.y);
+  wy = make_float2(s.a.z, s.a.w);
+  wz = make_float2(s.b.x, s.b.y);
+}
+__device__ __forceinline__ void get_w(const Stage<float>& s, float& wx, float& wy, float& wz) {
+  wx = s.a.x;
+  wy = s.a.z;
+  wz = s.b.x;
+}
+__device__ __forceinline__ void get_w(const Stage<double>& s, double& wx, double& wy, double& wz) {
+  wx = s.a.x;
+  wy = s.a.y;
+  wz = s.b.x;
+}
+
+// One lane's C columns of row p (p points at the lane's first column).
+template <class T, int C>
+__device__ __forceinline__ void load_v(const T* p, typename UK<T, C>::V (&v)[UK<T, C>::NV]) {
+  if constexpr (sizeof(T) == 4 && C == 4) {
+    const float4 q = __ldg(reinterpret_cast<const float4*>(p));
+    v[0] = make_float2(q.x, q.y);
+    v[1] = make_float2(q.z, q.w);
+  } else if constexpr (sizeof(T) == 4 && C == 2) {
+    v[0] = __ldg(reinterpret_cast<const float2*>(p));
+  } else if constexpr (sizeof(T) == 8 && C == 2) {
+    const double2 q = __ldg(reinterpret_cast<const double2*>(p));
+    v[0] = q.x;
+    v[1] = q.y;
+  } else {
+    v[0] = __ldg(p);
+  }
+}
+
+template <class T, int C>
+__device__ __forceinline__ void to_scalars(const typename UK<T, C>::V (&v)[UK<T, C>::NV], T (&s)[C]) {
+  if constexpr (sizeof(T) == 4 && C >= 2) {
+#pragma unroll
+    for (int k = 0; k < UK<T, C>::NV; ++k) {
+      s[2 * k] = v[k].x;
+      s[2 * k + 1] = v[k].y;
+    }
+  } else {
+#pragma unroll
+    for (int k = 0; k < C; ++k) s[k] = v[k];
+  }
+}
+
+template <class T, int C>
+__device__ __forceinline__ void load_s(const T* p, T (&s)[C]) {
+  typename UK<T, C>::V v[UK<T, C>::NV];
+  load_v<T, C>(p, v);
+  to_scalars<T, C>(v, s);
+}
+
+template <class T, int C>
+__device__ __forceinline__ void store_s(T* p, const T (&s)[C]) {
+  if constexpr (sizeof(T) == 4 && C == 4) {
+    *reinterpret_cast<float4*>(p) = make_float4(s[0], s[1], s[2], s[3]);
+  } else if constexpr (sizeof(T) == 4 && C == 2) {
+    *reinterpret_cast<float2*>(p) = make_float2(s[0], s[1]);
+  } else if constexpr (sizeof(T) == 8 && C == 2) {
+    *reinterpret_cast<double2*>(p) = make_double2(s[0], s[1]);
+  } else {
+    p[0] = s[0];
+  }
+}
+
+// X_j of union record rec for this lane's columns (Xc already offset to them);
+// off: lane outside a partial panel, nothing is read.
+template <class T, int C>
+__device__ __forceinline__ void gather_x(const T* Xc, int64_t ldx, uint32_t rec, bool on,
+                                         typename UK<T, C>::V (&x)[3][UK<T, C>::NV]) {
+  if (!on) return;
+  const T* p = Xc + 3 * (int64_t)(rec >> 8) * ldx;
+  load_v<T, C>(p, x[0]);
+  load_v<T, C>(p + ldx, x[1]);
+  load_v<T, C>(p + 2 * ldx, x[2]);
+}
+
+// Rows R0 + b for the set bits b of NIB, their w at sw[0], sw[1], ... in bit order.
+template <int R0, int NIB, class T, class V, int NV>
+__device__ __forceinline__ void nib_rows(V (&acc)[kTile][3][NV], const V (&x)[3][NV], const Stage<T>* sw) {
+  int idx = 0;
+#pragma unroll
+  for (int b = 0; b < 4; ++b) {
+    if (NIB & (1 << b)) {
+      V wx, wy, wz;
+      get_w(sw[idx], wx, wy, wz);
+#pragma unroll
+      for (int v = 0; v < NV; ++v) {
+        V d = vmul(wx, x[0][v]);
+        d = vfma(wy, x[1][v], d);
+        d = vfma(wz, x[2][v], d);
+        acc[R0 + b][0][v] = vfma(wx, d, acc[R0 + b][0][v]);
+        acc[R0 + b][1][v] = vfma(wy, d, acc[R0 + b][1][v]);
+        acc[R0 + b][2][v] = vfma(wz, d, acc[R0 + b][2][v]);
+      }
+      ++idx;
+    }
+  }
+}
+
+template <int R0, class T, class V, int NV>
+__device__ __forceinline__ void nib_dispatch(unsigned nib, V (&acc)[kTile][3][NV], const V (&x)[3][NV],
+                                             const Stage<T>* sw) {
+#define INCH_NIB(N)                        \
+  case N:                                  \
+    nib_rows<R0, N, T, V, NV>(acc, x, sw); \
+    break;
+  switch (nib) {
+    INCH_NIB(1)
+    INCH_NIB(2)
+    INCH_NIB(3)
+    INCH_NIB(4)
+    INCH_NIB(5)
+    INCH_NIB(6)
+    INCH_NIB(7)
+    INCH_NIB(8)
+    INCH_NIB(9)
+    INCH_NIB(10)
+    INCH_NIB(11)
+    INCH_NIB(12)
+    INCH_NIB(13)
+    INCH_NIB(14)
+    INCH_NIB(15)
+    default:
+      break;
+  }
+#undef INCH_NIB
+}
+
+template <class T>
+__device__ __forceinline__ void zero_val(T& a) {
+  a = T(0);
+}
+__device__ __forceinline__ void zero_val(float2& a) { a = make_float2(0.f, 0.f); }
+
+template <class T, int C>
+__global__ void __launch_bounds__(kWarpsUT * 32, UK<T, C>::MINB)
+k_spmm_band(int64_t n_atoms, const int64_t* __restrict__ uptr, const int64_t* __restrict__ pptr,
+            const uint32_t* __restrict__ urec, const void* __restrict__ pw, const T* __restrict__ diag,
+            const T* __restrict__ X, int64_t ldx, T* Y, int64_t ldy, const T* Yin, int64_t ldyin,
+            T* __restrict__ Acc, int64_t ldacc, int c0, int ncols, EpiT ep, const double* __restrict__ Q,
+            int64_t ndof, const double* __restrict__ coef) {
+  using V = typename UK<T, C>::V;
+  constexpr int NV = UK<T, C>::NV;
+  constexpr int P = 32 * C;
+  __shared__ Stage<T> s_w[kWarpsUT][kBatchPairs];
+  __shared__ double s_coef[8 * P];
   if (ep.r > 0) {
-    for (int t = threadIdx.x; t < ep.r * B; t += kThreads) s_coef[t] = coef[t];
+    for (int t = threadIdx.x; t < ep.r * P; t += kWarpsUT * 32) s_coef[t] = coef[t];
     __syncthreads();
   }
   const int lane = threadIdx.x & 31;
-  const int cl = lane % LPR;
-  const int grp = (threadIdx.x >> 5) * GPW + lane / LPR;
+  const int warp = threadIdx.x >> 5;
+  Stage<T>* sw = s_w[warp];
+  const bool on = lane * C < ncols;          // lane inside the panel
+  const T* Xc = X + c0 + lane * C;
   const int64_t ntiles = (n_atoms + kTile - 1) / kTile;
-  const int64_t per = (ntiles + gridDim.x - 1) / gridDim.x;
-  const int64_t t_beg = (int64_t)blockIdx.x * per;
-  const int64_t t_end = t_beg + per < ntiles ? t_beg + per : ntiles;
-  for (int64_t t = t_beg + grp; t < t_end; t += GPB) {
-    T acc[kTile][3][CPL][V];
+  for (int64_t t = (int64_t)blockIdx.x * kWarpsUT + warp; t < ntiles; t += (int64_t)gridDim.x * kWarpsUT) {
+    V acc[kTile][3][NV];
 #pragma unroll
     for (int r = 0; r < kTile; ++r)
 #pragma unroll
-      for (int q = 0; q < CPL; ++q)
+      for (int a = 0; a < 3; ++a)
 #pragma unroll
-        for (int v = 0; v < V; ++v) acc[r][0][q][v] = acc[r][1][q][v] = acc[r][2][q][v] = T(0);
-    int64_t p = pptr[t];
-    const int64_t u1 = uptr[t + 1];
-    const T* Xc = X + c0 + cl * V;
-    for (int64_t u = uptr[t]; u < u1; ++u) {
-      const uint32_t rec = __ldg(urec + u);
-      const int64_t j = rec >> 8;
-      const unsigned mask = rec & 0xffu;
-      const T* xj = Xc + 3 * j * ldx;
-      T x0[CPL][V], x1[CPL][V], x2[CPL][V];
+        for (int k = 0; k < NV; ++k) zero_val(acc[r][a][k]);
+    const int64_t u0 = uptr[t], u1 = uptr[t + 1];
+    int64_t pbase = pptr[t];
+    uint32_t rec = (u0 + lane < u1) ? __ldg(urec + u0 + lane) : 0u;
+    V xa[3][NV], xb[3][NV];
 #pragma unroll
-      for (int q = 0; q < CPL; ++q) {
-        vld2<T, V>(xj + q * LPR * V, x0[q]);
-        vld2<T, V>(xj + ldx + q * LPR * V, x1[q]);
-        vld2<T, V>(xj + 2 * ldx + q * LPR * V, x2[q]);
+    for (int a = 0; a < 3; ++a)
+#pragma unroll
+      for (int k = 0; k < NV; ++k) {
+        zero_val(xa[a][k]);
+        zero_val(xb[a][k]);
       }
+    gather_x<T, C>(Xc, ldx, __shfl_sync(0xffffffffu, rec, 0), on, xa);
+    gather_x<T, C>(Xc, ldx, __shfl_sync(0xffffffffu, rec, 1), on, xb);
+    for (int64_t ub = u0; ub < u1; ub += kUB) {
+      const int cnt = (int)((u1 - ub) < kUB ? (u1 - ub) : kUB);
+      const uint32_t recn = (ub + kUB + lane < u1) ? __ldg(urec + ub + kUB + lane) : 0u;
+      const int pc = __popc(rec & 0xffu);
+      int incl = pc;
 #pragma unroll
-      for (int r = 0; r < kTile; ++r) {
-        if (mask & (1u << r)) {
-          T wx, wy, wz;
-          PW<T>::load(pw, p, wx, wy, wz);
-          ++p;
-#pragma unroll
-          for (int q = 0; q < CPL; ++q)
-#pragma unroll
-            for (int v = 0; v < V; ++v) {
-              const T dot = wx * x0[q][v] + wy * x1[q][v] + wz * x2[q][v];
-              acc[r][0][q][v] -= wx * dot;
-              acc[r][1][q][v] -= wy * dot;
-              acc[r][2][q][v] -= wz * dot;
-            }
+      for (int o = 1; o < 32; o <<= 1) {
+        const int y = __shfl_up_sync(0xffffffffu, incl, o);
+        if (lane >= o) incl += y;
+      }
+      const int excl = incl - pc;
+      const int total = __shfl_sync(0xffffffffu, incl, 31);
+      __syncwarp();
+#pragma unroll 4
+      for (int s = lane; s < total; s += 32) Stage<T>::fill(sw + s, pw, pbase + s);
+      __syncwarp();
+      for (int k = 0; k < cnt; k += 2) {
+        {
+          const uint32_t rk = __shfl_sync(0xffffffffu, rec, k);
+          const int q = __shfl_sync(0xffffffffu, excl, k);
+          const unsigned m = rk & 0xffu;
+          nib_dispatch<0, T, V, NV>(m & 15u, acc, xa, sw + q);
+          nib_dispatch<4, T, V, NV>(m >> 4, acc, xa, sw + q + __popc(m & 15u));
+          const uint32_t ra = (k + 2 < kUB) ? __shfl_sync(0xffffffffu, rec, (k + 2) & 31)
+                                            : __shfl_sync(0xffffffffu, recn, (k + 2) & 31);
+          gather_x<T, C>(Xc, ldx, ra, on, xa);
+        }
+        if (k + 1 < cnt) {
+          const uint32_t rk = __shfl_sync(0xffffffffu, rec, k + 1);
+          const int q = __shfl_sync(0xffffffffu, excl, k + 1);
+          const unsigned m = rk & 0xffu;
+          nib_dispatch<0, T, V, NV>(m & 15u, acc, xb, sw + q);
+          nib_dispatch<4, T, V, NV>(m >> 4, acc, xb, sw + q + __popc(m & 15u));
+          const uint32_t rb = (k + 3 < kUB) ? __shfl_sync(0xffffffffu, rec, (k + 3) & 31)
+                                            : __shfl_sync(0xffffffffu, recn, (k + 3) & 31);
+          gather_x<T, C>(Xc, ldx, rb, on, xb);
         }
       }
+      pbase += total;
+      rec = recn;
     }
+    // epilogue: (H X)_i = D_i X_i - S_i, then the fused combination per element
 #pragma unroll
     for (int r = 0; r < kTile; ++r) {
       const int64_t i = t * kTile + r;
       if (i >= n_atoms) break;
+      if (!on) continue;
       const T* d = diag + 8 * i;
       const T dxx = d[0], dyy = d[1], dzz = d[2], dxy = d[3], dxz = d[4], dyz = d[5];
+      double al = ep.alpha, ga = ep.gamma, be = ep.beta;
+      if (ep.seg_coef != nullptr) {
+        const int sg = __ldg(ep.atom_seg + i);
+        al = __ldg(ep.seg_coef + 3 * sg);
+        ga = __ldg(ep.seg_coef + 3 * sg + 1);
+        be = __ldg(ep.seg_coef + 3 * sg + 2);
+      }
       const int64_t r0 = 3 * i;
+      T x0[C], x1[C], x2[C];
+      load_s<T, C>(Xc + r0 * ldx, x0);
+      load_s<T, C>(Xc + (r0 + 1) * ldx, x1);
+      load_s<T, C>(Xc + (r0 + 2) * ldx, x2);
+      T s0[C], s1[C], s2[C];
+      to_scalars<T, C>(acc[r][0], s0);
+      to_scalars<T, C>(acc[r][1], s1);
+      to_scalars<T, C>(acc[r][2], s2);
 #pragma unroll
-      for (int q = 0; q < CPL; ++q)
+      for (int a = 0; a < 3; ++a) {
+        const int64_t row = r0 + a;
+        T yv[C], yin[C];
+        if (ep.has_yin) load_s<T, C>(Yin + row * ldyin + c0 + lane * C, yin);
 #pragma unroll
-        for (int v = 0; v < V; ++v) {
-          const int c = (q * LPR + cl) * V + v;
-          const T x0 = X[r0 * ldx + c0 + c], x1 = X[(r0 + 1) * ldx + c0 + c], x2 = X[(r0 + 2) * ldx + c0 + c];
-          T h[3];
-          h[0] = acc[r][0][q][v] + dxx * x0 + dxy * x1 + dxz * x2;
-          h[1] = acc[r][1][q][v] + dxy * x0 + dyy * x1 + dyz * x2;
-          h[2] = acc[r][2][q][v] + dxz * x0 + dyz * x1 + dzz * x2;
-          const T xs[3] = {x0, x1, x2};
-#pragma unroll
-          for (int a = 0; a < 3; ++a) {
-            const int64_t row = r0 + a;
-            double y = ep.alpha * (double)h[a] + ep.gamma * (double)xs[a];
-            if (ep.has_yin) y += ep.beta * (double)Yin[row * ldyin + c0 + c];
-            for (int qq = 0; qq < ep.r; ++qq) y += Q[qq * ndof + row] * s_coef[qq * B + c];
-            Y[row * ldy + c0 + c] = (T)y;
-            if (ep.accumulate) Acc[row * ldacc + c0 + c] += (T)(ep.mu * y);
-          }
+        for (int c = 0; c < C; ++c) {
+          const T h = (a == 0)   ? (dxx * x0[c] + dxy * x1[c] + dxz * x2[c]) - s0[c]
+                      : (a == 1) ? (dxy * x0[c] + dyy * x1[c] + dyz * x2[c]) - s1[c]
+                                 : (dxz * x0[c] + dyz * x1[c] + dzz * x2[c]) - s2[c];
+          const T xa_ = (a == 0) ? x0[c] : (a == 1) ? x1[c] : x2[c];
+          double y = al * (double)h + ga * (double)xa_;
+          if (ep.has_yin) y += be * (double)yin[c];
+          for (int q = 0; q < ep.r; ++q) y += Q[q * ndof + row] * s_coef[q * P + lane * C + c];
+          yv[c] = (T)y;
         }
+        store_s<T, C>(Y + row * ldy + c0 + lane * C, yv);
+        if (ep.accumulate) {
+          T av[C];
+          load_s<T, C>(Acc + row * ldacc + c0 + lane * C, av);
+#pragma unroll
+          for (int c = 0; c < C; ++c) av[c] = (T)((double)av[c] + ep.mu * (double)yv[c]);
+          store_s<T, C>(Acc + row * ldacc + c0 + lane * C, av);
+        }
+      }
     }
   }
 }
 
-// Hotelling coefficients (same two-stage FP64 reduction as spmm.cu).
-template <class T, int B>
+constexpr int kThreads = 256;
+
+// Hotelling coefficients coef[q * P + c] = shift * sum_dof Q[q, dof] X[dof, c0 + c]
+// for the ncols columns of one panel: per-block partial sums, then one warp per
+// (q, c) adds the partials in a fixed order (deterministic, FP64).
+template <class T, int P>
 __global__ void __launch_bounds__(kThreads)
-k_qx_partial_t(const double* __restrict__ Q, int64_t ndof, const T* __restrict__ X, int64_t ldx, int c0,
+k_qx_partial_t(const double* __restrict__ Q, int64_t ndof, const T* __restrict__ X, int64_t ldx, int c0, int ncols,
                double* __restrict__ partial) {
   __shared__ double s[kThreads];
   const int q = blockIdx.y, r = gridDim.y;
   const double* qr = Q + q * ndof;
-  const int c = threadIdx.x % B;
+  const int c = threadIdx.x % P;
+  constexpr int RPB = kThreads / P;   // dofs per block step
   double acc = 0.0;
-  const int64_t total = ndof * B;
-  for (int64_t p = (int64_t)blockIdx.x * kThreads + threadIdx.x; p < total; p += (int64_t)gridDim.x * kThreads)
-    acc += qr[p / B] * (double)X[(p / B) * ldx + c0 + c];
+  if (c < ncols) {
+    for (int64_t dof = (int64_t)blockIdx.x * RPB + threadIdx.x / P; dof < ndof; dof += (int64_t)gridDim.x * RPB)
+      acc += qr[dof] * (double)X[dof * ldx + c0 + c];
+  }
   s[threadIdx.x] = acc;
   __syncthreads();
-  if (threadIdx.x < B) {
-    double t = 0.0;
-    for (int u = threadIdx.x; u < kThreads; u += B) t += s[u];
-    partial[((int64_t)blockIdx.x * r + q) * B + threadIdx.x] = t;
+  // tree over the threads of one column (P is a power of two dividing kThreads,
+  // so t and t + stride always share a column): log2(kThreads / P) steps
+#pragma unroll
+  for (int stride = kThreads / 2; stride >= P; stride >>= 1) {
+    if (threadIdx.x < stride) s[threadIdx.x] += s[threadIdx.x + stride];
+    __syncthreads();
   }
+  if (threadIdx.x < P) partial[((int64_t)blockIdx.x * r + q) * P + threadIdx.x] = s[threadIdx.x];
 }
 
-__global__ void k_qx_final_t(const double* __restrict__ partial, int P, int r, int B, double shift,
-                             double* __restrict__ coef) {
-  for (int t = threadIdx.x; t < r * B; t += blockDim.x) {
-    double s = 0.0;
-    for (int p = 0; p < P; ++p) s += partial[(int64_t)p * r * B + t];
-    coef[t] = shift * s;
-  }
+__global__ void __launch_bounds__(kThreads)
+k_qx_final_t(const double* __restrict__ partial, int nblk, int r, int P, double shift, double* __restrict__ coef) {
+  const int64_t t = (int64_t)blockIdx.x * (kThreads / 32) + (threadIdx.x >> 5);
+  if (t >= (int64_t)r * P) return;
+  const int lane = threadIdx.x & 31;
+  double s = 0.0;
+  for (int p = lane; p < nblk; p += 32) s += partial[(int64_t)p * r * P + t];
+  s = warp_sum(s);
+  if (lane == 0) coef[t] = shift * s;
 }
 
 constexpr int kQxBlocksT = 296;
 
-template <class T, int B>
-cudaError_t tile_launch(int64_t n, const int64_t* uptr, const int64_t* pptr, const uint32_t* urec, const void* pw,
+template <class T, int C>
+int band_grid(int64_t ntiles) {
+  static int per_sm = 0;
+  if (per_sm == 0) {
+    int nb = 0;
+    if (cudaOccupancyMaxActiveBlocksPerMultiprocessor(&nb, k_spmm_band<T, C>, kWarpsUT * 32, 0) != cudaSuccess ||
+        nb < 1)
+      nb = 1;
+    per_sm = nb;
+  }
+  int dev = 0, sms = 148;
+  if (cudaGetDevice(&dev) == cudaSuccess) cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev);
+  return grid_for(ntiles, kWarpsUT, sms * per_sm);
+}
+
+template <class T, int C>
+cudaError_t band_launch(int64_t n, const int64_t* uptr, const int64_t* pptr, const uint32_t* urec, const void* pw,
                         const T* diag, const T* X, int64_t ldx, T* Y, int64_t ldy, const T* Yin, int64_t ldyin,
-                        T* Acc, int64_t ldacc, int c0, EpiT ep, const double* Q, double hot_shift, double* partial,
-                        double* coef, cudaStream_t s) {
+                        T* Acc, int64_t ldacc, int c0, int ncols, EpiT ep, const double* Q, double hot_shift,
+                        double* partial, double* coef, cudaStream_t s) {
+  constexpr int P = 32 * C;
   const int64_t ndof = 3 * n;
   if (ep.r > 0) {
-    k_qx_partial_t<T, B><<<dim3(kQxBlocksT, ep.r), kThreads, 0, s>>>(Q, ndof, X, ldx, c0, partial);
-    k_qx_final_t<<<1, 512, 0, s>>>(partial, kQxBlocksT, ep.r, B, hot_shift, coef);
+    k_qx_partial_t<T, P><<<dim3(kQxBlocksT, ep.r), kThreads, 0, s>>>(Q, ndof, X, ldx, c0, ncols, partial);
+    const int outs = ep.r * P;
+    k_qx_final_t<<<(outs + kThreads / 32 - 1) / (kThreads / 32), kThreads, 0, s>>>(partial, kQxBlocksT, ep.r, P,
+                                                                                   hot_shift, coef);
   }
-  // float2 gathers only where a whole warp owns one tile (B = 64 in FP32); other
-  // widths use scalar gathers with 32 (or B) lanes per tile.
-  constexpr int VV = (sizeof(T) == 4 && B >= 64) ? 2 : 1;
-  const uintptr_t al = 2 * sizeof(T);
-  bool vec = (ldx % 2 == 0) && (ldy % 2 == 0) && (c0 % 2 == 0) && ((uintptr_t)X % al == 0) && ((uintptr_t)Y % al == 0);
-  if (ep.has_yin) vec = vec && (ldyin % 2 == 0) && ((uintptr_t)Yin % al == 0);
-  if (ep.accumulate) vec = vec && (ldacc % 2 == 0) && ((uintptr_t)Acc % al == 0);
   const int64_t ntiles = (n + kTile - 1) / kTile;
-  const int blocks = grid_for(ntiles, 32, 148 * 3);
-  if (VV == 2 && vec)
-    k_spmm_tiles<T, B, VV><<<blocks, kThreads, 0, s>>>(n, uptr, pptr, urec, pw, diag, X, ldx, Y, ldy, Yin, ldyin,
-                                                       Acc, ldacc, c0, ep, Q, ndof, coef);
-  else
-    k_spmm_tiles<T, B, 1><<<blocks, kThreads, 0, s>>>(n, uptr, pptr, urec, pw, diag, X, ldx, Y, ldy, Yin, ldyin,
-                                                      Acc, ldacc, c0, ep, Q, ndof, coef);
+  k_spmm_band<T, C><<<band_grid<T, C>(ntiles), kWarpsUT * 32, 0, s>>>(n, uptr, pptr, urec, pw, diag, X, ldx, Y, ldy,
+                                                                      Yin, ldyin, Acc, ldacc, c0, ncols, ep, Q,
+                                                                      ndof, coef);
   return cudaGetLastError();
+}
+
+// Process-wide choice of the widest FP32 panel (autotuner hook): 128 or 64.
+std::atomic<int> g_band_panel32{128};
+
+// Whether every vector operand allows loads/stores of `elems` elements per lane.
+template <class T>
+bool band_aligned(int elems, const T* X, int64_t ldx, const T* Y, int64_t ldy, const T* Yin, int64_t ldyin,
+                  const T* Acc, int64_t ldacc, int c0) {
+  const uintptr_t al = (uintptr_t)elems * sizeof(T);
+  bool ok = (ldx % elems == 0) && (ldy % elems == 0) && (c0 % elems == 0) && ((uintptr_t)X % al == 0) &&
+            ((uintptr_t)Y % al == 0);
+  if (Yin) ok = ok && (ldyin % elems == 0) && ((uintptr_t)Yin % al == 0);
+  if (Acc) ok = ok && (ldacc % elems == 0) && ((uintptr_t)Acc % al == 0);
+  return ok;
+}
+
+template <class T>
+cudaError_t band_run(int64_t n, const int64_t* uptr, const int64_t* pptr, const uint32_t* urec, const void* pw,
+                     const T* diag, const T* X, int64_t ldx, int b, T* Y, int64_t ldy, const T* Yin, int64_t ldyin,
+                     T* Acc, int64_t ldacc, EpiT ep, const double* Q, double hot_shift, double* partial,
+                     double* coef, cudaStream_t s) {
+  cudaError_t err = cudaSuccess;
+  int c0 = 0;
+  const T* Yin_ = ep.has_yin ? Yin : nullptr;
+  T* Acc_ = ep.accumulate ? Acc : nullptr;
+  while (c0 < b && err == cudaSuccess) {
+    const int rem = b - c0;
+    if constexpr (sizeof(T) == 4) {
+      const int widest = g_band_panel32.load();
+      if (widest >= 128 && rem >= 128 && band_aligned<T>(4, X, ldx, Y, ldy, Yin_, ldyin, Acc_, ldacc, c0)) {
+        err = band_launch<T, 4>(n, uptr, pptr, urec, pw, diag, X, ldx, Y, ldy, Yin, ldyin, Acc, ldacc, c0, 128, ep,
+                                Q, hot_shift, partial, coef, s);
+        c0 += 128;
+      } else if (rem >= 64 && band_aligned<T>(2, X, ldx, Y, ldy, Yin_, ldyin, Acc_, ldacc, c0)) {
+        err = band_launch<T, 2>(n, uptr, pptr, urec, pw, diag, X, ldx, Y, ldy, Yin, ldyin, Acc, ldacc, c0, 64, ep,
+                                Q, hot_shift, partial, coef, s);
+        c0 += 64;
+      } else {
+        const int nc = rem < 32 ? rem : 32;
+        err = band_launch<T, 1>(n, uptr, pptr, urec, pw, diag, X, ldx, Y, ldy, Yin, ldyin, Acc, ldacc, c0, nc, ep,
+                                Q, hot_shift, partial, coef, s);
+        c0 += nc;
+      }
+    } else {
+      if (rem >= 64 && band_aligned<T>(2, X, ldx, Y, ldy, Yin_, ldyin, Acc_, ldacc, c0)) {
+        err = band_launch<T, 2>(n, uptr, pptr, urec, pw, diag, X, ldx, Y, ldy, Yin, ldyin, Acc, ldacc, c0, 64, ep,
+                                Q, hot_shift, partial, coef, s);
+        c0 += 64;
+      } else {
+        const int nc = rem < 32 ? rem : 32;
+        err = band_launch<T, 1>(n, uptr, pptr, urec, pw, diag, X, ldx, Y, ldy, Yin, ldyin, Acc, ldacc, c0, nc, ep,
+                                Q, hot_shift, partial, coef, s);
+        c0 += nc;
+      }
+    }
+  }
+  return err;
 }
 
 }  // namespace
@@ -364,9 +671,16 @@ extern "C" inch_status inch_tile_store_fill(const double* X, int64_t n, double r
 
 extern "C" size_t inch_spmm_tiles_workspace_size(void) {
   Sizer s;
-  s.take<double>((size_t)kQxBlocksT * 8 * 64);
-  s.take<double>(8 * 64);
+  s.take<double>((size_t)kQxBlocksT * 8 * kMaxPanel);
+  s.take<double>(8 * kMaxPanel);
   return s.bytes();
+}
+
+extern "C" inch_status inch_spmm_band_tune(int32_t widest_fp32_panel) {
+  INCH_REQUIRE(widest_fp32_panel == 64 || widest_fp32_panel == 128, INCH_INVALID_ARG,
+               "inch_spmm_band_tune: widest FP32 panel must be 64 or 128");
+  g_band_panel32.store(widest_fp32_panel);
+  return INCH_OK;
 }
 
 extern "C" inch_status inch_spmm_tiles(int32_t prec, int64_t n, const int64_t* tile_uptr, const int64_t* tile_pptr,
@@ -378,7 +692,7 @@ extern "C" inch_status inch_spmm_tiles(int32_t prec, int64_t n, const int64_t* t
   INCH_REQUIRE(tile_uptr && tile_pptr && urec && pw && diag && Xv && Yv && ep_in, INCH_INVALID_ARG,
                "inch_spmm_tiles: NULL argument");
   INCH_REQUIRE(n >= 1 && n < (int64_t(1) << 24), INCH_INVALID_ARG, "inch_spmm_tiles: n_atoms out of range");
-  INCH_REQUIRE(b >= 1 && b <= 64, INCH_INVALID_ARG, "inch_spmm_tiles: b=%d outside 1..64", b);
+  INCH_REQUIRE(b >= 1, INCH_INVALID_ARG, "inch_spmm_tiles: b=%d below 1", b);
   INCH_REQUIRE(ldx >= b && ldy >= b && Xv != Yv, INCH_INVALID_ARG, "inch_spmm_tiles: bad leading dimension or X == Y");
   const inch_spmm_epilogue& e = *ep_in;
   INCH_REQUIRE(e.r >= 0 && e.r <= 8 && (e.r == 0 || q), INCH_INVALID_ARG, "inch_spmm_tiles: bad deflation basis");
@@ -389,39 +703,53 @@ extern "C" inch_status inch_spmm_tiles(int32_t prec, int64_t n, const int64_t* t
   double *partial = nullptr, *coef = nullptr;
   if (e.r > 0) {
     Carver c(ws, ws_bytes);
-    partial = c.take<double>((size_t)kQxBlocksT * 8 * 64);
-    coef = c.take<double>(8 * 64);
-    INCH_REQUIRE(c.ok, INCH_OOM, "inch_spmm_tiles: workspace too small");
+    partial = c.take<double>((size_t)kQxBlocksT * 8 * kMaxPanel);
+    coef = c.take<double>(8 * kMaxPanel);
+    INCH_REQUIRE(c.ok, INCH_OOM, "inch_spmm_tiles: workspace of %zu bytes, need %zu", ws_bytes,
+                 inch_spmm_tiles_workspace_size());
   }
-  EpiT ep{e.alpha, e.gamma, e.beta, e.mu, e.r, e.accumulate, e.beta != 0.0 ? 1 : 0};
-  cudaError_t err = cudaSuccess;
-  int c0 = 0;
-  while (c0 < b && err == cudaSuccess) {
-    const int rem = b - c0;
-#define TT(TYPE, BB)                                                                                         \
-  err = tile_launch<TYPE, BB>(n, tile_uptr, tile_pptr, urec, pw, static_cast<const TYPE*>(diag),              \
-                              static_cast<const TYPE*>(Xv), ldx, static_cast<TYPE*>(Yv), ldy,                  \
-                              static_cast<const TYPE*>(Yinv), ldyin, static_cast<TYPE*>(Accv), ldacc, c0, ep, q, \
-                              e.hot_shift, partial, coef, stream);                                             \
-  c0 += BB;
-    if (prec == 32) {
-      if (rem >= 64) { TT(float, 64) }
-      else if (rem >= 32) { TT(float, 32) }
-      else if (rem >= 16) { TT(float, 16) }
-      else if (rem >= 8) { TT(float, 8) }
-      else if (rem >= 4) { TT(float, 4) }
-      else if (rem >= 2) { TT(float, 2) }
-      else { TT(float, 1) }
-    } else {
-      if (rem >= 32) { TT(double, 32) }
-      else if (rem >= 16) { TT(double, 16) }
-      else if (rem >= 8) { TT(double, 8) }
-      else if (rem >= 4) { TT(double, 4) }
-      else if (rem >= 2) { TT(double, 2) }
-      else { TT(double, 1) }
-    }
-#undef TT
-  }
+  EpiT ep{e.alpha, e.gamma, e.beta, e.mu, e.r, e.accumulate, e.beta != 0.0 ? 1 : 0, nullptr, nullptr};
+  cudaError_t err;
+  if (prec == 32)
+    err = band_run<float>(n, tile_uptr, tile_pptr, urec, pw, static_cast<const float*>(diag),
+                          static_cast<const float*>(Xv), ldx, b, static_cast<float*>(Yv), ldy,
+                          static_cast<const float*>(Yinv), ldyin, static_cast<float*>(Accv), ldacc, ep, q,
+                          e.hot_shift, partial, coef, stream);
+  else
+    err = band_run<double>(n, tile_uptr, tile_pptr, urec, pw, static_cast<const double*>(diag),
+                           static_cast<const double*>(Xv), ldx, b, static_cast<double*>(Yv), ldy,
+                           static_cast<const double*>(Yinv), ldyin, static_cast<double*>(Accv), ldacc, ep, q,
+                           e.hot_shift, partial, coef, stream);
   INCH_REQUIRE(err == cudaSuccess, INCH_CUDA_ERROR, "inch_spmm_tiles: %s", cudaGetErrorString(err));
+  return INCH_OK;
+}
+
+extern "C" inch_status inch_spmm_tiles_seg(int32_t prec, int64_t n, const int64_t* tile_uptr,
+                                           const int64_t* tile_pptr, const uint32_t* urec, const void* pw,
+                                           const void* diag, const void* Xv, int64_t ldx, int32_t b, void* Yv,
+                                           int64_t ldy, const void* Yinv, int64_t ldyin, const int32_t* atom_seg,
+                                           const double* seg_coef, cudaStream_t stream) {
+  INCH_REQUIRE(prec == 32 || prec == 64, INCH_INVALID_ARG, "inch_spmm_tiles_seg: prec must be 32 or 64");
+  INCH_REQUIRE(tile_uptr && tile_pptr && urec && pw && diag && Xv && Yv && atom_seg && seg_coef, INCH_INVALID_ARG,
+               "inch_spmm_tiles_seg: NULL argument");
+  INCH_REQUIRE(n >= 1 && n < (int64_t(1) << 24), INCH_INVALID_ARG, "inch_spmm_tiles_seg: n_atoms out of range");
+  INCH_REQUIRE(b >= 1 && ldx >= b && ldy >= b && Xv != Yv, INCH_INVALID_ARG,
+               "inch_spmm_tiles_seg: bad b / leading dimension / aliasing");
+  INCH_REQUIRE(Yinv == nullptr || ldyin >= b, INCH_INVALID_ARG, "inch_spmm_tiles_seg: ldyin below b");
+  INCH_REQUIRE(((uintptr_t)pw & 15) == 0 && ((uintptr_t)diag & 15) == 0, INCH_INVALID_ARG,
+               "inch_spmm_tiles_seg: store buffers must be 16-byte aligned");
+  EpiT ep{0.0, 0.0, 0.0, 0.0, 0, 0, Yinv != nullptr ? 1 : 0, seg_coef, atom_seg};
+  cudaError_t err;
+  if (prec == 32)
+    err = band_run<float>(n, tile_uptr, tile_pptr, urec, pw, static_cast<const float*>(diag),
+                          static_cast<const float*>(Xv), ldx, b, static_cast<float*>(Yv), ldy,
+                          static_cast<const float*>(Yinv), ldyin, nullptr, 0, ep, nullptr, 0.0, nullptr, nullptr,
+                          stream);
+  else
+    err = band_run<double>(n, tile_uptr, tile_pptr, urec, pw, static_cast<const double*>(diag),
+                           static_cast<const double*>(Xv), ldx, b, static_cast<double*>(Yv), ldy,
+                           static_cast<const double*>(Yinv), ldyin, nullptr, 0, ep, nullptr, 0.0, nullptr, nullptr,
+                           stream);
+  INCH_REQUIRE(err == cudaSuccess, INCH_CUDA_ERROR, "inch_spmm_tiles_seg: %s", cudaGetErrorString(err));
   return INCH_OK;
 }

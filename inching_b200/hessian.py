@@ -50,7 +50,7 @@ class HessianStore:
     order the caller wants (normally reversed Cuthill-McKee)."""
 
     def __init__(self, X_nm, rc_gamma_A: float = 8.0, plus_i: float = 1.0, precisions=("f64", "f32"),
-                 device=None, graph_=None, tiles=False, pair_weight=None, pbc=None):
+                 device=None, graph_=None, tiles="auto", pair_weight=None, pbc=None, keep_pairs=True):
         self.X = graph.to_device_coords(X_nm, device)
         self.device = self.X.device
         self.n_atoms = int(self.X.shape[0])
@@ -63,8 +63,15 @@ class HessianStore:
         self.image = graph_[3] if len(graph_) > 3 else None
         if (self.box_xy is None) != (self.image is None):
             raise AssertionError("ABORTED. periodic images need both the box and the image codes of the lists")
+        if tiles == "auto":
+            # the band-tile layout takes neither periodic images nor per-pair springs
+            tiles = self.box_xy is None and pair_weight is None and self.n_atoms < (1 << 24)
         if self.box_xy is not None and tiles:
             raise AssertionError("ABORTED. the row-tile layout does not take periodic images")
+        if pair_weight is not None and tiles:
+            raise AssertionError("ABORTED. the row-tile layout does not take per-pair spring constants")
+        if not keep_pairs and not tiles:
+            raise AssertionError("ABORTED. keep_pairs=False needs the row-tile layout")
         want64 = "f64" in precisions
         want32 = "f32" in precisions
         self.ent64, self.diag64, self.ent32, self.diag32 = _native.hessian_assemble(
@@ -83,6 +90,12 @@ class HessianStore:
             uptr, pptr, urec, pw64, pw32, nu, npairs = _native.tile_store(self.X, self.rowptr, self.cols,
                                                                           self.rc_nm, want64, want32)
             self.tiles = dict(uptr=uptr, pptr=pptr, urec=urec, pw64=pw64, pw32=pw32, n_union=nu, n_pairs=npairs)
+            if not keep_pairs:
+                # every product goes through the band tiles; the pair entries are freed
+                # (the diagonal blocks stay: both layouts use them)
+                self.ent64 = None if self.ent64 is None else self.ent64[:0]
+                self.ent32 = None if self.ent32 is None else self.ent32[:0]
+        self.keep_pairs = bool(keep_pairs)
 
     # -- reference-compatible views ------------------------------------------------
     @property
@@ -111,7 +124,7 @@ class HessianStore:
         else the pair layout (entries + diagonal + rowptr)."""
         ent, diag = self.store(prec)
         dbytes = diag.numel() * diag.element_size()
-        if b >= 8 and self.tiles is not None and self.use_tiles:
+        if self._tiled(prec, b):
             t = self.tiles
             pw = t["pw64"] if prec == 64 else t["pw32"]
             return (t["n_union"] * 4 + t["n_pairs"] * pw.shape[1] * pw.element_size()
@@ -126,8 +139,8 @@ class HessianStore:
         want = torch.float64 if prec == 64 else torch.float32
         if X.dtype != want:
             raise AssertionError(f"ABORTED. prec {prec} needs {want} vectors, got {X.dtype}")
-        if (X.dim() == 2 and X.shape[1] >= 8 and X.shape[1] % 8 != 0 and epilogue.get("Yin") is None
-                and epilogue.get("acc") is None):
+        if (not self._tiled(prec, 1 if X.dim() == 1 else X.shape[1]) and X.dim() == 2 and X.shape[1] >= 8
+                and X.shape[1] % 8 != 0 and epilogue.get("Yin") is None and epilogue.get("acc") is None):
             # pad the block to a multiple of 8 columns so every column tile runs the
             # vector-gather kernel on aligned rows; the zero columns cost < 8 columns
             b = X.shape[1]
@@ -153,24 +166,33 @@ class HessianStore:
             ev0.record()
             out = self._matmul(prec, ent, diag, X, out, epilogue)
             ev1.record()
-            probe.records.append((ev0, ev1, nbytes, _launches(b, prec)))
+            nl = _native.band_panels(prec, b) if self._tiled(prec, b) else _launches(b, prec)
+            probe.records.append((ev0, ev1, nbytes, nl))
             return out
         return self._matmul(prec, ent, diag, X, out, epilogue)
 
+    def _tiled(self, prec, b):
+        """Whether a b-column product at this precision runs on the band tiles: always
+        when the pair entries were dropped, else for b >= 8 (narrower products keep
+        the pair kernel, whose lanes split a row's entries)."""
+        if self.tiles is None or not self.use_tiles:
+            return False
+        if (self.tiles["pw64"] if prec == 64 else self.tiles["pw32"]) is None:
+            return False
+        return b >= 8 or not self.keep_pairs
+
     def _matmul(self, prec, ent, diag, X, out, epilogue):
-        if X.dim() == 2 and X.shape[1] >= 8 and self.tiles is not None and self.use_tiles:
+        b = 1 if X.dim() == 1 else X.shape[1]
+        if self._tiled(prec, b):
             t = self.tiles
             pw = t["pw64"] if prec == 64 else t["pw32"]
-            if pw is not None:
-                for c0 in range(0, X.shape[1], 64):
-                    sl = slice(c0, min(c0 + 64, X.shape[1]))
-                    kw = dict(epilogue)
-                    for key in ("Yin", "acc"):
-                        if kw.get(key) is not None:
-                            kw[key] = kw[key][:, sl]
-                    _native.spmm_tiles(prec, self.n_atoms, t["uptr"], t["pptr"], t["urec"], pw, diag, X[:, sl],
-                                       out[:, sl], **kw)
+            if X.dim() == 1:
+                kw = {k: (v[:, None] if (k in ("Yin", "acc") and v is not None) else v) for k, v in epilogue.items()}
+                _native.spmm_tiles(prec, self.n_atoms, t["uptr"], t["pptr"], t["urec"], pw, diag, X[:, None],
+                                   out[:, None], **kw)
                 return out
+            _native.spmm_tiles(prec, self.n_atoms, t["uptr"], t["pptr"], t["urec"], pw, diag, X, out, **epilogue)
+            return out
         if X.dim() == 1 or X.shape[1] <= 64:
             return _native.spmm(prec, self.n_atoms, self.rowptr, ent, diag, X, out, **epilogue)
         # the kernel takes up to 64 columns per call: walk column panels
@@ -187,6 +209,11 @@ class HessianStore:
         """out = alpha_s (H X) + gamma_s X + beta_s Yin with per-segment coefficients
         (block-diagonal stores of many structures; pair layout)."""
         ent, diag = self.store(prec)
+        if self._tiled(prec, X.shape[1]):
+            t = self.tiles
+            pw = t["pw64"] if prec == 64 else t["pw32"]
+            return _native.spmm_tiles_seg(prec, self.n_atoms, t["uptr"], t["pptr"], t["urec"], pw, diag, X, out,
+                                          atom_seg, seg_coef, Yin=Yin)
         for c0 in range(0, X.shape[1], 64):
             sl = slice(c0, min(c0 + 64, X.shape[1]))
             _native.spmm_seg(prec, self.n_atoms, self.rowptr, ent, diag, X[:, sl], out[:, sl], atom_seg, seg_coef,

@@ -7,8 +7,11 @@
  *     tensor's data_ptr); *_host is host memory.
  *   - Every entry point takes the cudaStream_t it enqueues on.  Entry points that
  *     must read a size back to the host say "synchronises" and do so on that stream.
- *   - The library never frees caller memory and never allocates device memory:
- *     scratch comes from a caller-provided workspace whose size is queried first.
+ *   - The library never frees caller memory.  Kernel scratch comes from a
+ *     caller-provided workspace whose size is queried first.  The one device
+ *     allocation the library makes itself is cuBLAS's: the solver building blocks
+ *     (inch_block_orth, inch_rr_project, inch_rr_rotate) create one cuBLAS handle
+ *     per device on first use, which allocates cuBLAS's own internal state.
  *   - Return value: INCH_OK or an error code; inch_last_error_string() gives a
  *     message for the calling thread's last error.
  *   - Coordinates are float64 nanometres, atoms in caller order; degrees of
@@ -222,7 +225,8 @@ inch_status inch_mp_adam(float* w, const float* g, float* m1, float* m2, int64_t
  * where Q is the (r, 3N) row-major FP64 deflation basis (r <= 8; explicit
  * Hotelling deflation); its coefficients Q X are reduced inside the call.
  * Yin may alias Y.  prec: 64 -> f64 store and f64 vectors; 32 -> f32 store and
- * f32 vectors.  Supported b: 1..64 (f32) / 1..32 (f64).
+ * f32 vectors.  Supported b: 1..64 at both precisions (FP64 runs 64 columns as
+ * two 32-column tiles).
  * ------------------------------------------------------------------------- */
 typedef struct {
   double alpha, gamma, beta, mu, hot_shift;
@@ -348,12 +352,32 @@ inch_status inch_tile_store_fill(const double* X_dev, int64_t n_atoms, double rc
                                  const int64_t* tile_pptr_dev, uint32_t* urec_dev, double* pw64_dev,
                                  float* pw32_dev, cudaStream_t stream);
 size_t inch_spmm_tiles_workspace_size(void);
+/* The band-tile product: one warp per 8-row tile and column panel (FP32 panels of
+ * 128 columns with the packed f32x2 FMAs of sm_100, or 64 / 32; FP64 panels of
+ * 64 / 32), each union column's X_j gathered once for all rows of its mask.
+ * Any b >= 1 (the library walks the panels; b < 32 runs one partial panel).
+ * Replaces the same two cuSPARSE SpMVs as inch_spmm (Burn/Krylov/T3.py:138-156),
+ * with the same fused epilogue.  Vector rows whose leading dimensions and column
+ * offset are multiples of 4 (FP32) or 2 elements take the vector panels; any
+ * other alignment runs scalar panels.  ws: inch_spmm_tiles_workspace_size()
+ * bytes, used only when ep->r > 0. */
 inch_status inch_spmm_tiles(int32_t prec, int64_t n_atoms, const int64_t* tile_uptr_dev,
                             const int64_t* tile_pptr_dev, const uint32_t* urec_dev, const void* pw_dev,
                             const void* diag_dev, const void* X_dev, int64_t ldx, int32_t b,
                             void* Y_dev, int64_t ldy, const void* Yin_dev, int64_t ldyin,
                             void* Acc_dev, int64_t ldacc, const double* q_dev,
                             const inch_spmm_epilogue* ep, void* ws_dev, size_t ws_bytes, cudaStream_t stream);
+/* inch_spmm_seg on the band tiles (per-segment alpha, gamma, beta; any b >= 1).
+ * Used by the CUDA-graph Chebyshev filter, whose coefficients live in a device
+ * table (PolynomialFilters/T2.py:59-80 as one graph replay). */
+inch_status inch_spmm_tiles_seg(int32_t prec, int64_t n_atoms, const int64_t* tile_uptr_dev,
+                                const int64_t* tile_pptr_dev, const uint32_t* urec_dev, const void* pw_dev,
+                                const void* diag_dev, const void* X_dev, int64_t ldx, int32_t b,
+                                void* Y_dev, int64_t ldy, const void* Yin_dev, int64_t ldyin,
+                                const int32_t* atom_seg_dev, const double* seg_coef_dev, cudaStream_t stream);
+/* Widest FP32 panel of the band-tile product for this process (128 or 64): the
+ * autotuner's hook (no reference counterpart). */
+inch_status inch_spmm_band_tune(int32_t widest_fp32_panel);
 
 /* Allocation-free form of inch_spmm (no counterpart in the reference).  For
  * callers that cannot provide device scratch -- hosts running on another
@@ -361,10 +385,14 @@ inch_status inch_spmm_tiles(int32_t prec, int64_t n_atoms, const int64_t* tile_u
  * bindings that own only their input and output buffers -- the deflation partial
  * sums live in a static device array of about 1.2 MB held by every GPU that
  * loads the library until exit.  Limits: b <= 64 columns and r <= 8 deflation
- * vectors (else INCH_LIMIT).  The first call on a device looks up the array's
- * device address (cudaGetSymbolAddress); make that first call before any stream
- * capture.  All calls share the array: calls that overlap on the GPU race and
- * must be serialised by the caller.  Allocates nothing. */
+ * vectors (else INCH_LIMIT).  The array is used only when ep->r > 0: the first
+ * such call on a device looks up the array's device address
+ * (cudaGetSymbolAddress) and keeps it for the process; make that first call
+ * before any stream capture.  The kept address is not refreshed after a
+ * cudaDeviceReset, so a caller that resets a device must not call this entry
+ * point on it afterwards.  All calls share the array: calls with r > 0 that
+ * overlap on the GPU race and must be serialised by the caller.  Allocates
+ * nothing. */
 inch_status inch_spmm_noalloc(int32_t prec, int64_t n_atoms, const int64_t* rowptr_dev,
                               const void* ent_dev, const void* diag_dev,
                               const void* X_dev, int64_t ldx, int32_t b,
