@@ -3,11 +3,13 @@
 Run from the repository root with the reference checkout available:
 
     python tests/golden/make_golden.py /path/to/Inching
+    python tests/golden/make_golden.py /path/to/Inching hessian    # dense Hessians only
 
 It imports InchingLiteInteger's k-d-tree Cuthill-McKee ordering, its ungapped
 band-slice routine and its Chebyshev filter design (numpy/scipy only; the
 unused openmm/mdtraj/matplotlib imports of util.py are stubbed) and stores their
-outputs on seeded synthetic inputs as small .npz files.  Nothing at test time
+outputs on seeded synthetic inputs as small .npz files.  The "hessian" step runs
+the reference's dense torch Hessian (Burn/Coordinate/T3.py) on the CPU.  Nothing at test time
 reads the reference; the tests only read these files.
 """
 from __future__ import annotations
@@ -171,5 +173,60 @@ def main(ref_root):
     print("polyfilter", len(windows) * 4)
 
 
+def dense_hessian_reference(ref_root, X_nm, rc_nm, plus_i):
+    """The reference's dense torch Hessian, X_D_K_Hessian (InchingLiteInteger/Burn/
+    Coordinate/T3.py:47-127), on the CPU: D = pairwise distances, Gamma = 1 within
+    the cutoff by cKDTree's rule (self included; the reference zeroes the self
+    term through nan_to_num), accumulation in float64.  Its arithmetic runs unchanged; only its
+    CUDA-only housekeeping is replaced for the CPU: torch.device(0) maps to the CPU,
+    TorchMakePrecision sets the default dtype alone (not the CUDA tensor type) and
+    TorchEmptyCache does nothing."""
+    import torch
+    for m in ["openmm", "openmm.app", "mdtraj", "matplotlib", "matplotlib.pyplot"]:
+        sys.modules.setdefault(m, types.ModuleType(m))
+    sys.path.insert(0, ref_root)
+    import InchingLiteInteger.util as rutil                      # noqa
+    import InchingLiteInteger.Burn.Coordinate.T3 as dense        # noqa
+    saved = (torch.device, rutil.TorchMakePrecision, rutil.TorchEmptyCache, torch.get_default_dtype())
+    real_device = torch.device
+    try:
+        dense.torch.device = lambda *a, **k: real_device("cpu")
+        rutil.TorchMakePrecision = lambda Precision="torch.float64": torch.set_default_dtype(
+            {"torch.float64": torch.float64, "torch.float32": torch.float32}[str(Precision)])
+        rutil.TorchEmptyCache = lambda: None
+        Xn = np.ascontiguousarray(X_nm, dtype=np.float64)
+        dif = Xn[None, :, :] - Xn[:, None, :]
+        d2 = (dif[..., 0] * dif[..., 0] + dif[..., 1] * dif[..., 1]) + dif[..., 2] * dif[..., 2]
+        X = torch.from_numpy(Xn)
+        D = torch.from_numpy(np.sqrt(d2))
+        # the cutoff graph by cKDTree's rule (squared distance in this order, <= rc^2)
+        Gamma = torch.from_numpy((d2 <= rc_nm * rc_nm).astype(np.float64))
+        H = _quiet(dense.X_D_K_Hessian, X, D, Gamma, maxleafsize=100, PlusI=plus_i, dtype_temp=torch.float64)
+    finally:
+        torch.device, rutil.TorchMakePrecision, rutil.TorchEmptyCache = saved[:3]
+        torch.set_default_dtype(saved[3])
+    return H.numpy()
+
+
+def hessian_goldens(ref_root):
+    """Dense reference Hessians on two seeded structures (the edge-case structure of
+    near_cutoff_structure and a 400-atom globule), stored as their lower triangle
+    (incl. diagonal) in COO form: rows, cols int32, vals float64."""
+    meta = dict(numpy=np.__version__, scipy=scipy.__version__)
+    import torch
+    meta["torch"] = torch.__version__
+    cases = {"near_cutoff": near_cutoff_structure(), "globule400": synth.globule(400, seed=31) / 10.0}
+    for name, X in cases.items():
+        H = dense_hessian_reference(ref_root, X, 0.8, 1.0)
+        r, c = np.nonzero(np.tril(H))
+        np.savez_compressed(os.path.join(HERE, f"hessian_{name}.npz"), X=X, rc_nm=np.float64(0.8),
+                            plus_i=np.float64(1.0), rows=r.astype(np.int32), cols=c.astype(np.int32),
+                            vals=H[r, c], n=np.int64(H.shape[0]), **meta)
+        print("hessian", name, X.shape[0], "nnz(lower)", len(r))
+
+
 if __name__ == "__main__":
+    if len(sys.argv) > 2 and sys.argv[2] == "hessian":
+        hessian_goldens(sys.argv[1])
+        sys.exit(0)
     main(sys.argv[1] if len(sys.argv) > 1 else os.environ.get("INCHING_REFERENCE", "../Inching"))

@@ -150,3 +150,27 @@ def test_row_tile_layout_matches_oracle(case, prec, b):
               Q=torch.from_numpy(Q).cuda(), hot_shift=10.0)
     tol = (TOL64 if prec == 64 else TOL32) * abs(Hfull).max() * np.abs(Xv).max() * 50
     assert np.abs(Yt.double().cpu().numpy() - ref).max() <= tol
+
+
+@pytest.mark.parametrize("name", ["near_cutoff", "globule400"])
+def test_store_matches_reference_dense_hessian(name):
+    """The CUDA store (FP64 pair entries and, through products, the band tiles)
+    against the reference's own dense Hessian X_D_K_Hessian (Burn/Coordinate/
+    T3.py:47-127), stored by tests/golden/make_golden.py: 1e-12 of its largest entry."""
+    from inching_b200.hessian import HessianStore
+    g = np.load(f"tests/golden/hessian_{name}.npz")
+    n = int(g["n"])
+    L = np.zeros((n, n))
+    L[g["rows"], g["cols"]] = g["vals"]
+    Href = L + np.tril(L, -1).T
+    H = HessianStore(g["X"], float(g["rc_nm"]) * 10.0, plus_i=float(g["plus_i"]), tiles=True)
+    Lh = H.to_scipy_lower().toarray()
+    Hs = Lh + np.tril(Lh, -1).T
+    scale = np.abs(Href).max()
+    assert np.abs(Hs - Href).max() <= TOL64 * scale
+    # products through the band tiles: H e_k for a block of unit vectors = columns of Href
+    E = torch.zeros((n, 40), dtype=torch.float64, device="cuda")
+    cols = np.arange(0, n, max(1, n // 40))[:40]
+    E[torch.from_numpy(cols).cuda(), torch.arange(len(cols), device="cuda")] = 1.0
+    Y = H.matmul(E).cpu().numpy()
+    assert np.abs(Y[:, :len(cols)] - Href[:, cols]).max() <= TOL64 * scale
