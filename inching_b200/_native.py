@@ -111,7 +111,7 @@ _SIGS = {
     "inch_spmm_tiles_seg": (ctypes.c_int, [c_int32, c_int64, c_void_p, c_void_p, c_void_p, c_void_p, c_void_p,
                                            c_void_p, c_int64, c_int32, c_void_p, c_int64, c_void_p, c_int64,
                                            c_void_p, c_void_p, c_void_p]),
-    "inch_spmm_band_tune": (ctypes.c_int, [c_int32]),
+    "inch_spmm_band_tune": (ctypes.c_int, [c_int32, c_int32]),
     "inch_hessian_assemble_weighted": (ctypes.c_int, [c_void_p, c_int64, c_double, c_double, c_void_p, c_void_p,
                                                       c_void_p, c_void_p, c_void_p, c_void_p, c_void_p, c_void_p]),
     "inch_mp_edge_concat": (ctypes.c_int, [c_void_p, c_void_p, c_void_p, c_int64, c_int32, c_int32, c_void_p,
@@ -427,10 +427,11 @@ def band_panels(prec, b):
     return n + (rem + 31) // 32
 
 
-def spmm_band_tune(widest_fp32_panel=128):
-    """Widest FP32 panel of the band-tile product for this process: 128 or 64."""
+def spmm_band_tune(widest_fp32_panel=128, ring_depth=8):
+    """Band-tile launch choices for this process: widest FP32 panel (128 or 64) and
+    the staging ring depth per warp (4, 8 or 16)."""
     global _band_widest32
-    check(lib().inch_spmm_band_tune(widest_fp32_panel))
+    check(lib().inch_spmm_band_tune(widest_fp32_panel, ring_depth))
     _band_widest32 = int(widest_fp32_panel)
 
 

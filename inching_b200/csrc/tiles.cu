@@ -101,28 +101,28 @@ __global__ void k_set0_pair(int64_t* a, int64_t* b) {
 }
 
 // ---------------------------------------------------------------------------
-// Band-tile product (union walk).
+// Band-tile product (union walk through a shared-memory ring).
 //
 // One warp owns one 8-row tile and one column panel of P = 32*C columns; lane l
 // owns the C consecutive columns [l*C, l*C + C) of the panel.  The tile's union
-// records arrive 32 at a time (one coalesced load; the next batch is loaded one
-// batch ahead), an exclusive warp scan of popc(mask) gives each union column's
-// first pair, and the batch's w (at most 256 pairs) is staged once in this
-// warp's slice of shared memory, so every pair reads its w as one broadcast
-// shared load.  X_j of union column u is gathered once (three coalesced row
-// segments of P values) two columns ahead of its use (two register sets, A for
-// even and B for odd union columns) and applied to every row of the mask.  The
-// mask is split in two nibbles; each nibble dispatches through a 16-way switch
-// to straight-line code with the accumulator rows fixed at compile time, so the
-// accumulators stay in registers and no per-row bit test is executed.
+// records arrive 32 at a time (one coalesced load, the next batch one batch
+// ahead, with its exclusive scan of popc(mask) giving each union column's first
+// pair).  Union column u is staged kRing - 1 columns ahead of its use in a
+// per-warp ring of kRing stages by cp.async: each lane copies its own C columns
+// of the three rows of X_j (lane-private, cached in L1 for the neighbouring
+// tiles of the other warps), and lanes 0..popc(mask)-1 copy the column's w
+// values.  So each warp keeps kRing - 1 gathers in flight without holding them
+// in registers.  The row mask is split in two nibbles; each nibble dispatches
+// through a 16-way switch to straight-line code with the accumulator rows fixed
+// at compile time, so the accumulators stay in registers and no per-row bit
+// test is executed.
 //
 // FP32 panels with C >= 2 use the packed f32x2 FMAs of sm_100 (two columns per
-// instruction); the staged w is stored pre-broadcast ({wx,wx,wy,wy},{wz,wz,0,0})
-// so that its halves are the f32x2 operands directly.  The accumulators hold
-// S = sum_j w (w . X_j); the epilogue forms (H X)_i = D_i X_i - S.
+// instruction).  The accumulators hold S = sum_j w (w . X_j); the epilogue forms
+// (H X)_i = D_i X_i - S.
 // ---------------------------------------------------------------------------
 constexpr int kUB = 32;                    // union records per batch
-constexpr int kBatchPairs = kUB * kTile;   // pairs of one batch, at most
+constexpr int kRingDefault = 8;            // ring stages per warp (power of two; 4, 8 or 16)
 constexpr int kWarpsUT = 4;                // warps per block
 constexpr int kMaxPanel = 128;             // widest panel (FP32, C = 4)
 
@@ -133,25 +133,24 @@ struct EpiT {
   const int* atom_seg;
 };
 
+// w of one pair as stored by the tile store: FP32 {wx,wy,wz,0}, FP64 the same in doubles.
 template <class T>
-struct Stage;
+struct WRaw;
 template <>
-struct Stage<float> {
-  float4 a, b;   // {wx,wx,wy,wy}, {wz,wz,0,0}
-  __device__ __forceinline__ static void fill(Stage* s, const void* pw, int64_t p) {
-    const float4 v = __ldg(reinterpret_cast<const float4*>(pw) + p);
-    s->a = make_float4(v.x, v.x, v.y, v.y);
-    s->b = make_float4(v.z, v.z, 0.f, 0.f);
-  }
+struct WRaw<float> {
+  float4 v;
 };
 template <>
-struct Stage<double> {
-  double2 a, b;  // {wx,wy}, {wz,0}
-  __device__ __forceinline__ static void fill(Stage* s, const void* pw, int64_t p) {
-    const double2* q = reinterpret_cast<const double2*>(pw) + 2 * p;
-    s->a = __ldg(q);
-    s->b = __ldg(q + 1);
-  }
+struct WRaw<double> {
+  double2 a, b;
+};
+
+// One ring stage: this warp's slice of X_j (3 rows x P columns) and the w of the
+// union column's pairs (at most kTile).
+template <class T, int C>
+struct RingStage {
+  T x[3][32 * C];
+  WRaw<T> w[kTile];
 };
 
 // Register vector type of one lane's columns: NV values of type V.
@@ -195,37 +194,58 @@ __device__ __forceinline__ float vfma(float a, float b, float c) { return fmaf(a
 __device__ __forceinline__ double vmul(double a, double b) { return a * b; }
 __device__ __forceinline__ double vfma(double a, double b, double c) { return fma(a, b, c); }
 
-__device__ __forceinline__ void get_w(const Stage<float>& s, float2& wx, float2& wy, float2& wz) {
-  wx = make_float2(s.a.x, s.a.y);
-  wy = make_float2(s.a.z, s.a.w);
-  wz = make_float2(s.b.x, s.b.y);
+__device__ __forceinline__ void get_w(const WRaw<float>& s, float2& wx, float2& wy, float2& wz) {
+  const float4 v = s.v;
+  wx = make_float2(v.x, v.x);
+  wy = make_float2(v.y, v.y);
+  wz = make_float2(v.z, v.z);
 }
-__device__ __forceinline__ void get_w(const Stage<float>& s, float& wx, float& wy, float& wz) {
-  wx = s.a.x;
-  wy = s.a.z;
-  wz = s.b.x;
+__device__ __forceinline__ void get_w(const WRaw<float>& s, float& wx, float& wy, float& wz) {
+  const float4 v = s.v;
+  wx = v.x;
+  wy = v.y;
+  wz = v.z;
 }
-__device__ __forceinline__ void get_w(const Stage<double>& s, double& wx, double& wy, double& wz) {
-  wx = s.a.x;
-  wy = s.a.y;
-  wz = s.b.x;
+__device__ __forceinline__ void get_w(const WRaw<double>& s, double& wx, double& wy, double& wz) {
+  const double2 a = s.a, b = s.b;
+  wx = a.x;
+  wy = a.y;
+  wz = b.x;
 }
 
-// One lane's C columns of row p (p points at the lane's first column).
-template <class T, int C>
+// cp.async of N bytes global -> shared (N in {4, 8, 16}; both addresses N-aligned).
+template <int N>
+__device__ __forceinline__ void cp_async(void* smem, const void* gmem) {
+  const unsigned s = static_cast<unsigned>(__cvta_generic_to_shared(smem));
+  if constexpr (N == 16)
+    asm volatile("cp.async.ca.shared.global [%0], [%1], 16;\n" ::"r"(s), "l"(gmem) : "memory");
+  else if constexpr (N == 8)
+    asm volatile("cp.async.ca.shared.global [%0], [%1], 8;\n" ::"r"(s), "l"(gmem) : "memory");
+  else
+    asm volatile("cp.async.ca.shared.global [%0], [%1], 4;\n" ::"r"(s), "l"(gmem) : "memory");
+}
+__device__ __forceinline__ void cp_async_commit() { asm volatile("cp.async.commit_group;\n" ::: "memory"); }
+template <int N>
+__device__ __forceinline__ void cp_async_wait() {
+  asm volatile("cp.async.wait_group %0;\n" ::"n"(N) : "memory");
+}
+
+// One lane's C columns of row p (p points at the lane's first column), from
+// global (__ldg) or shared memory.
+template <class T, int C, bool GLOBAL>
 __device__ __forceinline__ void load_v(const T* p, typename UK<T, C>::V (&v)[UK<T, C>::NV]) {
   if constexpr (sizeof(T) == 4 && C == 4) {
-    const float4 q = __ldg(reinterpret_cast<const float4*>(p));
+    const float4 q = GLOBAL ? __ldg(reinterpret_cast<const float4*>(p)) : *reinterpret_cast<const float4*>(p);
     v[0] = make_float2(q.x, q.y);
     v[1] = make_float2(q.z, q.w);
   } else if constexpr (sizeof(T) == 4 && C == 2) {
-    v[0] = __ldg(reinterpret_cast<const float2*>(p));
+    v[0] = GLOBAL ? __ldg(reinterpret_cast<const float2*>(p)) : *reinterpret_cast<const float2*>(p);
   } else if constexpr (sizeof(T) == 8 && C == 2) {
-    const double2 q = __ldg(reinterpret_cast<const double2*>(p));
+    const double2 q = GLOBAL ? __ldg(reinterpret_cast<const double2*>(p)) : *reinterpret_cast<const double2*>(p);
     v[0] = q.x;
     v[1] = q.y;
   } else {
-    v[0] = __ldg(p);
+    v[0] = GLOBAL ? __ldg(p) : *p;
   }
 }
 
@@ -246,7 +266,7 @@ __device__ __forceinline__ void to_scalars(const typename UK<T, C>::V (&v)[UK<T,
 template <class T, int C>
 __device__ __forceinline__ void load_s(const T* p, T (&s)[C]) {
   typename UK<T, C>::V v[UK<T, C>::NV];
-  load_v<T, C>(p, v);
+  load_v<T, C, true>(p, v);
   to_scalars<T, C>(v, s);
 }
 
@@ -263,21 +283,9 @@ __device__ __forceinline__ void store_s(T* p, const T (&s)[C]) {
   }
 }
 
-// X_j of union record rec for this lane's columns (Xc already offset to them);
-// off: lane outside a partial panel, nothing is read.
-template <class T, int C>
-__device__ __forceinline__ void gather_x(const T* Xc, int64_t ldx, uint32_t rec, bool on,
-                                         typename UK<T, C>::V (&x)[3][UK<T, C>::NV]) {
-  if (!on) return;
-  const T* p = Xc + 3 * (int64_t)(rec >> 8) * ldx;
-  load_v<T, C>(p, x[0]);
-  load_v<T, C>(p + ldx, x[1]);
-  load_v<T, C>(p + 2 * ldx, x[2]);
-}
-
 // Rows R0 + b for the set bits b of NIB, their w at sw[0], sw[1], ... in bit order.
 template <int R0, int NIB, class T, class V, int NV>
-__device__ __forceinline__ void nib_rows(V (&acc)[kTile][3][NV], const V (&x)[3][NV], const Stage<T>* sw) {
+__device__ __forceinline__ void nib_rows(V (&acc)[kTile][3][NV], const V (&x)[3][NV], const WRaw<T>* sw) {
   int idx = 0;
 #pragma unroll
   for (int b = 0; b < 4; ++b) {
@@ -300,7 +308,7 @@ __device__ __forceinline__ void nib_rows(V (&acc)[kTile][3][NV], const V (&x)[3]
 
 template <int R0, class T, class V, int NV>
 __device__ __forceinline__ void nib_dispatch(unsigned nib, V (&acc)[kTile][3][NV], const V (&x)[3][NV],
-                                             const Stage<T>* sw) {
+                                             const WRaw<T>* sw) {
 #define INCH_NIB(N)                        \
   case N:                                  \
     nib_rows<R0, N, T, V, NV>(acc, x, sw); \
@@ -333,7 +341,25 @@ __device__ __forceinline__ void zero_val(T& a) {
 }
 __device__ __forceinline__ void zero_val(float2& a) { a = make_float2(0.f, 0.f); }
 
-template <class T, int C>
+// Exclusive scan of popc(mask) over the 32 records of a batch; total in `tot`.
+__device__ __forceinline__ int batch_scan(uint32_t rec, int lane, int& tot) {
+  const int pc = __popc(rec & 0xffu);
+  int incl = pc;
+#pragma unroll
+  for (int o = 1; o < 32; o <<= 1) {
+    const int y = __shfl_up_sync(0xffffffffu, incl, o);
+    if (lane >= o) incl += y;
+  }
+  tot = __shfl_sync(0xffffffffu, incl, 31);
+  return incl - pc;
+}
+
+template <class T, int C, int kRing>
+constexpr size_t band_smem_bytes() {
+  return (size_t)kWarpsUT * kRing * sizeof(RingStage<T, C>);
+}
+
+template <class T, int C, int kRing>
 __global__ void __launch_bounds__(kWarpsUT * 32, UK<T, C>::MINB)
 k_spmm_band(int64_t n_atoms, const int64_t* __restrict__ uptr, const int64_t* __restrict__ pptr,
             const uint32_t* __restrict__ urec, const void* __restrict__ pw, const T* __restrict__ diag,
@@ -341,9 +367,12 @@ k_spmm_band(int64_t n_atoms, const int64_t* __restrict__ uptr, const int64_t* __
             T* __restrict__ Acc, int64_t ldacc, int c0, int ncols, EpiT ep, const double* __restrict__ Q,
             int64_t ndof, const double* __restrict__ coef) {
   using V = typename UK<T, C>::V;
+  using St = RingStage<T, C>;
   constexpr int NV = UK<T, C>::NV;
   constexpr int P = 32 * C;
-  __shared__ Stage<T> s_w[kWarpsUT][kBatchPairs];
+  constexpr int XB = C * (int)sizeof(T);          // bytes of one lane's slice of one row
+  constexpr int WB = (int)sizeof(WRaw<T>);         // bytes of one pair's w
+  extern __shared__ __align__(16) unsigned char band_smem[];
   __shared__ double s_coef[8 * P];
   if (ep.r > 0) {
     for (int t = threadIdx.x; t < ep.r * P; t += kWarpsUT * 32) s_coef[t] = coef[t];
@@ -351,9 +380,10 @@ k_spmm_band(int64_t n_atoms, const int64_t* __restrict__ uptr, const int64_t* __
   }
   const int lane = threadIdx.x & 31;
   const int warp = threadIdx.x >> 5;
-  Stage<T>* sw = s_w[warp];
+  St* ring = reinterpret_cast<St*>(band_smem) + warp * kRing;
   const bool on = lane * C < ncols;          // lane inside the panel
   const T* Xc = X + c0 + lane * C;
+  const unsigned char* pwb = static_cast<const unsigned char*>(pw);
   const int64_t ntiles = (n_atoms + kTile - 1) / kTile;
   for (int64_t t = (int64_t)blockIdx.x * kWarpsUT + warp; t < ntiles; t += (int64_t)gridDim.x * kWarpsUT) {
     V acc[kTile][3][NV];
@@ -364,58 +394,68 @@ k_spmm_band(int64_t n_atoms, const int64_t* __restrict__ uptr, const int64_t* __
 #pragma unroll
         for (int k = 0; k < NV; ++k) zero_val(acc[r][a][k]);
     const int64_t u0 = uptr[t], u1 = uptr[t + 1];
+    // batch at ub (rec, excl, tot) and the next one (recn, excln, totn)
+    int64_t ub = u0;
     int64_t pbase = pptr[t];
     uint32_t rec = (u0 + lane < u1) ? __ldg(urec + u0 + lane) : 0u;
-    V xa[3][NV], xb[3][NV];
-#pragma unroll
-    for (int a = 0; a < 3; ++a)
-#pragma unroll
-      for (int k = 0; k < NV; ++k) {
-        zero_val(xa[a][k]);
-        zero_val(xb[a][k]);
-      }
-    gather_x<T, C>(Xc, ldx, __shfl_sync(0xffffffffu, rec, 0), on, xa);
-    gather_x<T, C>(Xc, ldx, __shfl_sync(0xffffffffu, rec, 1), on, xb);
-    for (int64_t ub = u0; ub < u1; ub += kUB) {
-      const int cnt = (int)((u1 - ub) < kUB ? (u1 - ub) : kUB);
-      const uint32_t recn = (ub + kUB + lane < u1) ? __ldg(urec + ub + kUB + lane) : 0u;
-      const int pc = __popc(rec & 0xffu);
-      int incl = pc;
-#pragma unroll
-      for (int o = 1; o < 32; o <<= 1) {
-        const int y = __shfl_up_sync(0xffffffffu, incl, o);
-        if (lane >= o) incl += y;
-      }
-      const int excl = incl - pc;
-      const int total = __shfl_sync(0xffffffffu, incl, 31);
-      __syncwarp();
-#pragma unroll 4
-      for (int s = lane; s < total; s += 32) Stage<T>::fill(sw + s, pw, pbase + s);
-      __syncwarp();
-      for (int k = 0; k < cnt; k += 2) {
-        {
-          const uint32_t rk = __shfl_sync(0xffffffffu, rec, k);
-          const int q = __shfl_sync(0xffffffffu, excl, k);
-          const unsigned m = rk & 0xffu;
-          nib_dispatch<0, T, V, NV>(m & 15u, acc, xa, sw + q);
-          nib_dispatch<4, T, V, NV>(m >> 4, acc, xa, sw + q + __popc(m & 15u));
-          const uint32_t ra = (k + 2 < kUB) ? __shfl_sync(0xffffffffu, rec, (k + 2) & 31)
-                                            : __shfl_sync(0xffffffffu, recn, (k + 2) & 31);
-          gather_x<T, C>(Xc, ldx, ra, on, xa);
+    int tot;
+    int excl = batch_scan(rec, lane, tot);
+    uint32_t recn = (u0 + kUB + lane < u1) ? __ldg(urec + u0 + kUB + lane) : 0u;
+    int totn;
+    int excln = batch_scan(recn, lane, totn);
+    // stage union gg (gg - ub < 2 * kUB) into its ring slot
+    auto issue = [&](int64_t gg) {
+      if (gg < u1) {
+        const int li = (int)(gg - ub);
+        uint32_t rr;
+        int64_t q;
+        if (li < kUB) {
+          rr = __shfl_sync(0xffffffffu, rec, li);
+          q = pbase + __shfl_sync(0xffffffffu, excl, li);
+        } else {
+          rr = __shfl_sync(0xffffffffu, recn, li - kUB);
+          q = pbase + tot + __shfl_sync(0xffffffffu, excln, li - kUB);
         }
-        if (k + 1 < cnt) {
-          const uint32_t rk = __shfl_sync(0xffffffffu, rec, k + 1);
-          const int q = __shfl_sync(0xffffffffu, excl, k + 1);
-          const unsigned m = rk & 0xffu;
-          nib_dispatch<0, T, V, NV>(m & 15u, acc, xb, sw + q);
-          nib_dispatch<4, T, V, NV>(m >> 4, acc, xb, sw + q + __popc(m & 15u));
-          const uint32_t rb = (k + 3 < kUB) ? __shfl_sync(0xffffffffu, rec, (k + 3) & 31)
-                                            : __shfl_sync(0xffffffffu, recn, (k + 3) & 31);
-          gather_x<T, C>(Xc, ldx, rb, on, xb);
+        St* st = ring + ((gg - u0) & (kRing - 1));
+        if (on) {
+          const T* p = Xc + 3 * (int64_t)(rr >> 8) * ldx;
+          cp_async<XB>(&st->x[0][lane * C], p);
+          cp_async<XB>(&st->x[1][lane * C], p + ldx);
+          cp_async<XB>(&st->x[2][lane * C], p + 2 * ldx);
+        }
+        if (lane < __popc(rr & 0xffu)) {
+          const unsigned char* src = pwb + (q + lane) * WB;
+          unsigned char* dst = reinterpret_cast<unsigned char*>(&st->w[lane]);
+#pragma unroll
+          for (int o = 0; o < WB; o += 16) cp_async<16>(dst + o, src + o);
         }
       }
-      pbase += total;
-      rec = recn;
+      cp_async_commit();
+    };
+#pragma unroll
+    for (int s = 0; s < kRing - 1; ++s) issue(u0 + s);
+    for (int64_t g = u0; g < u1; ++g) {
+      if (g - ub == kUB) {              // next batch of records
+        ub += kUB;
+        pbase += tot;
+        rec = recn;
+        excl = excln;
+        tot = totn;
+        recn = (ub + kUB + lane < u1) ? __ldg(urec + ub + kUB + lane) : 0u;
+        excln = batch_scan(recn, lane, totn);
+      }
+      __syncwarp();                     // every lane is done with the slot issue() refills
+      issue(g + kRing - 1);
+      cp_async_wait<kRing - 1>();       // this lane's copies of union g have landed
+      __syncwarp();                     // ... and every other lane's (the w values)
+      const St* st = ring + ((g - u0) & (kRing - 1));
+      const unsigned m = __shfl_sync(0xffffffffu, rec, (int)(g - ub)) & 0xffu;
+      V x[3][NV];
+      load_v<T, C, false>(&st->x[0][lane * C], x[0]);
+      load_v<T, C, false>(&st->x[1][lane * C], x[1]);
+      load_v<T, C, false>(&st->x[2][lane * C], x[2]);
+      nib_dispatch<0, T, V, NV>(m & 15u, acc, x, st->w);
+      nib_dispatch<4, T, V, NV>(m >> 4, acc, x, st->w + __popc(m & 15u));
     }
     // epilogue: (H X)_i = D_i X_i - S_i, then the fused combination per element
 #pragma unroll
@@ -468,6 +508,7 @@ k_spmm_band(int64_t n_atoms, const int64_t* __restrict__ uptr, const int64_t* __
       }
     }
   }
+  cp_async_wait<0>();   // nothing of this warp's may still be in flight at exit
 }
 
 constexpr int kThreads = 256;
@@ -514,12 +555,21 @@ k_qx_final_t(const double* __restrict__ partial, int nblk, int r, int P, double 
 
 constexpr int kQxBlocksT = 296;
 
-template <class T, int C>
+// Process-wide launch choices (autotuner hooks): the widest FP32 panel (128 or
+// 64 columns) and the ring depth (4, 8 or 16 union columns per warp).
+std::atomic<int> g_band_panel32{128};
+std::atomic<int> g_band_ring{kRingDefault};
+
+// Grid of the band kernel: its resident blocks per SM (registers and the ring's
+// dynamic shared memory, opted in once per instantiation) times the SM count.
+template <class T, int C, int R>
 int band_grid(int64_t ntiles) {
   static int per_sm = 0;
   if (per_sm == 0) {
     int nb = 0;
-    if (cudaOccupancyMaxActiveBlocksPerMultiprocessor(&nb, k_spmm_band<T, C>, kWarpsUT * 32, 0) != cudaSuccess ||
+    const size_t sm = band_smem_bytes<T, C, R>();
+    cudaFuncSetAttribute(k_spmm_band<T, C, R>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sm);
+    if (cudaOccupancyMaxActiveBlocksPerMultiprocessor(&nb, k_spmm_band<T, C, R>, kWarpsUT * 32, sm) != cudaSuccess ||
         nb < 1)
       nb = 1;
     per_sm = nb;
@@ -543,14 +593,22 @@ cudaError_t band_launch(int64_t n, const int64_t* uptr, const int64_t* pptr, con
                                                                                    hot_shift, coef);
   }
   const int64_t ntiles = (n + kTile - 1) / kTile;
-  k_spmm_band<T, C><<<band_grid<T, C>(ntiles), kWarpsUT * 32, 0, s>>>(n, uptr, pptr, urec, pw, diag, X, ldx, Y, ldy,
-                                                                      Yin, ldyin, Acc, ldacc, c0, ncols, ep, Q,
-                                                                      ndof, coef);
+#define INCH_BAND(R)                                                                                       \
+  k_spmm_band<T, C, R><<<band_grid<T, C, R>(ntiles), kWarpsUT * 32, band_smem_bytes<T, C, R>(), s>>>(        \
+      n, uptr, pptr, urec, pw, diag, X, ldx, Y, ldy, Yin, ldyin, Acc, ldacc, c0, ncols, ep, Q, ndof, coef);
+  const int ring = g_band_ring.load();
+  if (ring == 4) {
+    INCH_BAND(4)
+  } else if (ring == 16) {
+    INCH_BAND(16)
+  } else {
+    INCH_BAND(8)
+  }
+#undef INCH_BAND
   return cudaGetLastError();
 }
 
-// Process-wide choice of the widest FP32 panel (autotuner hook): 128 or 64.
-std::atomic<int> g_band_panel32{128};
+
 
 // Whether every vector operand allows loads/stores of `elems` elements per lane.
 template <class T>
@@ -676,10 +734,13 @@ extern "C" size_t inch_spmm_tiles_workspace_size(void) {
   return s.bytes();
 }
 
-extern "C" inch_status inch_spmm_band_tune(int32_t widest_fp32_panel) {
+extern "C" inch_status inch_spmm_band_tune(int32_t widest_fp32_panel, int32_t ring_depth) {
   INCH_REQUIRE(widest_fp32_panel == 64 || widest_fp32_panel == 128, INCH_INVALID_ARG,
                "inch_spmm_band_tune: widest FP32 panel must be 64 or 128");
+  INCH_REQUIRE(ring_depth == 4 || ring_depth == 8 || ring_depth == 16, INCH_INVALID_ARG,
+               "inch_spmm_band_tune: ring depth must be 4, 8 or 16");
   g_band_panel32.store(widest_fp32_panel);
+  g_band_ring.store(ring_depth);
   return INCH_OK;
 }
 

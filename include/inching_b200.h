@@ -375,9 +375,10 @@ inch_status inch_spmm_tiles_seg(int32_t prec, int64_t n_atoms, const int64_t* ti
                                 const void* diag_dev, const void* X_dev, int64_t ldx, int32_t b,
                                 void* Y_dev, int64_t ldy, const void* Yin_dev, int64_t ldyin,
                                 const int32_t* atom_seg_dev, const double* seg_coef_dev, cudaStream_t stream);
-/* Widest FP32 panel of the band-tile product for this process (128 or 64): the
- * autotuner's hook (no reference counterpart). */
-inch_status inch_spmm_band_tune(int32_t widest_fp32_panel);
+/* Launch choices of the band-tile product for this process: the widest FP32
+ * panel (128 or 64 columns) and the depth of each warp's staging ring (4, 8 or
+ * 16 union columns in flight).  The autotuner's hook (no reference counterpart). */
+inch_status inch_spmm_band_tune(int32_t widest_fp32_panel, int32_t ring_depth);
 
 /* Allocation-free form of inch_spmm (no counterpart in the reference).  For
  * callers that cannot provide device scratch -- hosts running on another

@@ -54,21 +54,23 @@ def test_band_product_matches_krylov_av(case, prec, b):
     assert np.abs(Y.double().cpu().numpy() - ref).max() <= tol
 
 
-@pytest.mark.parametrize("widest", [128, 64])
-def test_band_fp32_panel_choice_same_product(case, widest):
-    """The autotuner's panel switch (128- or 64-column FP32 panels) changes the
-    launch shape, not the product."""
+@pytest.mark.parametrize("widest,ring", [(128, 8), (64, 8), (128, 4), (64, 16), (128, 16)])
+@pytest.mark.parametrize("prec", [64, 32])
+def test_band_launch_choice_same_product(case, widest, ring, prec):
+    """The autotuner's switches (128- or 64-column FP32 panels, ring depth 4, 8 or
+    16) change the launch shape, not the product."""
     from inching_b200 import _native
     Xr, H, A, Ad, scale, Q = case
     rng = np.random.default_rng(5)
-    Xv = rng.standard_normal((H.shape[0], 256))
+    Xv = rng.standard_normal((H.shape[0], 200))
     ref = _ref(A, Ad, Xv)
+    dt = torch.float64 if prec == 64 else torch.float32
     try:
-        _native.spmm_band_tune(widest)
-        Y = H.matmul(torch.from_numpy(Xv).to("cuda", torch.float32).contiguous(), prec=32)
+        _native.spmm_band_tune(widest, ring)
+        Y = H.matmul(torch.from_numpy(Xv).to("cuda", dt).contiguous(), prec=prec)
     finally:
-        _native.spmm_band_tune(128)
-    assert np.abs(Y.double().cpu().numpy() - ref).max() <= TOL[32] * scale * np.abs(Xv).max() * 10
+        _native.spmm_band_tune(128, 8)
+    assert np.abs(Y.double().cpu().numpy() - ref).max() <= TOL[prec] * scale * np.abs(Xv).max() * 10
 
 
 @pytest.mark.parametrize("prec", [64, 32])
