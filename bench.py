@@ -64,8 +64,6 @@ def parse():
     ap.add_argument("--layout", default="tiles", choices=["tiles", "pairs"], help="store layout for --kernel-only")
     ap.add_argument("--band-panel", type=int, default=None, choices=[64, 128],
                     help="widest FP32 panel of the band-tile product (--kernel-only)")
-    ap.add_argument("--band-ring", type=int, default=8, choices=[4, 8, 16],
-                    help="staging ring depth of the band-tile product (--kernel-only)")
     return ap.parse_args()
 
 
@@ -80,8 +78,8 @@ def run_kernel_only(args):
     if args.tune:
         t, bps = (int(x) for x in args.tune.split(","))
         _native.spmm_tune(t, bps)
-    if args.band_panel or args.band_ring != 8:
-        _native.spmm_band_tune(args.band_panel or 128, args.band_ring)
+    if args.band_panel:
+        _native.spmm_band_tune(args.band_panel)
     Xd = torch.from_numpy(synth.workload(args.workload) / 10.0).cuda()
     order, _ = graph.cuthill_mckee(Xd, 8.0)
     prec = 32 if args.kernel_only == "spmm32" else 64
@@ -102,7 +100,7 @@ def run_kernel_only(args):
     nbytes = H.store_bytes(prec, args.b) + 2 * X.numel() * X.element_size()
     best = min(ms)
     print(json.dumps({"kernel": args.kernel_only, "b": args.b, "tune": args.tune, "layout": args.layout,
-                      "band_panel": args.band_panel, "band_ring": args.band_ring, "n_atoms": H.n_atoms,
+                      "band_panel": args.band_panel, "n_atoms": H.n_atoms,
                       "nnz": H.nnz_blocks,
                       "ms": [round(m, 4) for m in ms], "algorithmic_bytes": nbytes,
                       "best_GBps": round(nbytes / best / 1e6, 1)}))

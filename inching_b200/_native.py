@@ -111,7 +111,8 @@ _SIGS = {
     "inch_spmm_tiles_seg": (ctypes.c_int, [c_int32, c_int64, c_void_p, c_void_p, c_void_p, c_void_p, c_void_p,
                                            c_void_p, c_int64, c_int32, c_void_p, c_int64, c_void_p, c_int64,
                                            c_void_p, c_void_p, c_void_p]),
-    "inch_spmm_band_tune": (ctypes.c_int, [c_int32, c_int32]),
+    "inch_spmm_band_tune": (ctypes.c_int, [c_int32]),
+    "inch_spmm_band_status": (ctypes.c_int, [POINTER(c_int32)]),
     "inch_hessian_assemble_weighted": (ctypes.c_int, [c_void_p, c_int64, c_double, c_double, c_void_p, c_void_p,
                                                       c_void_p, c_void_p, c_void_p, c_void_p, c_void_p, c_void_p]),
     "inch_mp_edge_concat": (ctypes.c_int, [c_void_p, c_void_p, c_void_p, c_int64, c_int32, c_int32, c_void_p,
@@ -427,12 +428,19 @@ def band_panels(prec, b):
     return n + (rem + 31) // 32
 
 
-def spmm_band_tune(widest_fp32_panel=128, ring_depth=8):
-    """Band-tile launch choices for this process: widest FP32 panel (128 or 64) and
-    the staging ring depth per warp (4, 8 or 16)."""
+def spmm_band_tune(widest_fp32_panel=128):
+    """Widest FP32 panel of the band-tile product for this process: 128 or 64."""
     global _band_widest32
-    check(lib().inch_spmm_band_tune(widest_fp32_panel, ring_depth))
+    check(lib().inch_spmm_band_tune(widest_fp32_panel))
     _band_widest32 = int(widest_fp32_panel)
+
+
+def spmm_band_status():
+    """0, or 1 if a band-tile launch since the last call stopped at a bounded wait
+    (synchronises; reading clears it)."""
+    v = c_int32(0)
+    check(lib().inch_spmm_band_status(ctypes.byref(v)))
+    return int(v.value)
 
 
 def spmm_tiles_seg(prec, n_atoms, uptr, pptr, urec, pw, diag, X, Y, atom_seg, seg_coef, Yin=None):

@@ -101,30 +101,37 @@ __global__ void k_set0_pair(int64_t* a, int64_t* b) {
 }
 
 // ---------------------------------------------------------------------------
-// Band-tile product (union walk through a shared-memory ring).
+// Band-tile product (union walk, TMA-staged batches).
 //
 // One warp owns one 8-row tile and one column panel of P = 32*C columns; lane l
 // owns the C consecutive columns [l*C, l*C + C) of the panel.  The tile's union
-// records arrive 32 at a time (one coalesced load, the next batch one batch
-// ahead, with its exclusive scan of popc(mask) giving each union column's first
-// pair).  Union column u is staged kRing - 1 columns ahead of its use in a
-// per-warp ring of kRing stages by cp.async: each lane copies its own C columns
-// of the three rows of X_j (lane-private, cached in L1 for the neighbouring
-// tiles of the other warps), and lanes 0..popc(mask)-1 copy the column's w
-// values.  So each warp keeps kRing - 1 gathers in flight without holding them
-// in registers.  The row mask is split in two nibbles; each nibble dispatches
-// through a 16-way switch to straight-line code with the accumulator rows fixed
-// at compile time, so the accumulators stay in registers and no per-row bit
-// test is executed.
+// columns are processed in batches of kBatch.  A batch is staged in this warp's
+// slice of shared memory by the bulk-copy (TMA) engine: lane u (< kBatch) issues
+// the three row segments of X_j for union column u of the batch (P values each,
+// rows 3j, 3j+1, 3j+2), lane kBatch issues one copy of the batch's w values
+// (contiguous in the tile store), and all of them complete on the buffer's
+// mbarrier.  Batches are double-buffered: batch b+1 is in flight while batch b
+// is multiplied, so a warp keeps up to 2*kBatch gathers outstanding while its
+// lanes execute only arithmetic and shared loads.
 //
-// FP32 panels with C >= 2 use the packed f32x2 FMAs of sm_100 (two columns per
-// instruction).  The accumulators hold S = sum_j w (w . X_j); the epilogue forms
-// (H X)_i = D_i X_i - S.
+// For each union column, each lane reads its slice of X_j once and applies it to
+// every row of the column's mask.  The mask is split in two nibbles; each nibble
+// dispatches through a 16-way switch to straight-line code with the accumulator
+// rows fixed at compile time, so the accumulators stay in registers.  FP32
+// panels with C >= 2 use the packed f32x2 FMAs of sm_100.  The accumulators hold
+// S = sum_j w (w . X_j); the epilogue forms (H X)_i = D_i X_i - S.
+//
+// Every mbarrier wait is bounded; a wait that runs out records kBandTimeout in
+// the status word (read by inch_spmm_band_status) and the warp stops after
+// draining its outstanding copies.
 // ---------------------------------------------------------------------------
-constexpr int kUB = 32;                    // union records per batch
-constexpr int kRingDefault = 8;            // ring stages per warp (power of two; 4, 8 or 16)
+constexpr int kBatch = 8;                  // union columns per staged batch
 constexpr int kWarpsUT = 4;                // warps per block
 constexpr int kMaxPanel = 128;             // widest panel (FP32, C = 4)
+constexpr unsigned kWaitSpins = 1u << 24;  // bound of one mbarrier wait
+constexpr int kBandTimeout = 1;
+
+__device__ int g_band_status;              // 0, or kBandTimeout after a wait ran out
 
 struct EpiT {
   double alpha, gamma, beta, mu;
@@ -145,12 +152,18 @@ struct WRaw<double> {
   double2 a, b;
 };
 
-// One ring stage: this warp's slice of X_j (3 rows x P columns) and the w of the
-// union column's pairs (at most kTile).
+// One staged batch: this warp's slice of X_j (3 rows x P columns) for kBatch
+// union columns and the w of their pairs (at most kTile each).
 template <class T, int C>
-struct RingStage {
-  T x[3][32 * C];
-  WRaw<T> w[kTile];
+struct Batch {
+  T x[kBatch][3][32 * C];
+  WRaw<T> w[kBatch * kTile];
+};
+
+template <class T, int C>
+struct WarpSmem {
+  Batch<T, C> buf[2];
+  unsigned long long bar[2];
 };
 
 // Register vector type of one lane's columns: NV values of type V.
@@ -160,7 +173,7 @@ template <>
 struct UK<float, 4> {
   using V = float2;
   static constexpr int NV = 2;
-  static constexpr int MINB = 3;
+  static constexpr int MINB = 2;
 };
 template <>
 struct UK<float, 2> {
@@ -178,7 +191,7 @@ template <>
 struct UK<double, 2> {
   using V = double;
   static constexpr int NV = 2;
-  static constexpr int MINB = 3;
+  static constexpr int MINB = 2;
 };
 template <>
 struct UK<double, 1> {
@@ -213,25 +226,40 @@ __device__ __forceinline__ void get_w(const WRaw<double>& s, double& wx, double&
   wz = b.x;
 }
 
-// cp.async of N bytes global -> shared (N in {4, 8, 16}; both addresses N-aligned).
-template <int N>
-__device__ __forceinline__ void cp_async(void* smem, const void* gmem) {
-  const unsigned s = static_cast<unsigned>(__cvta_generic_to_shared(smem));
-  if constexpr (N == 16)
-    asm volatile("cp.async.ca.shared.global [%0], [%1], 16;\n" ::"r"(s), "l"(gmem) : "memory");
-  else if constexpr (N == 8)
-    asm volatile("cp.async.ca.shared.global [%0], [%1], 8;\n" ::"r"(s), "l"(gmem) : "memory");
-  else
-    asm volatile("cp.async.ca.shared.global [%0], [%1], 4;\n" ::"r"(s), "l"(gmem) : "memory");
+// --- mbarrier and bulk-copy helpers (this CTA's shared memory only) ----------
+__device__ __forceinline__ unsigned smem_u32(const void* p) {
+  return static_cast<unsigned>(__cvta_generic_to_shared(p));
 }
-__device__ __forceinline__ void cp_async_commit() { asm volatile("cp.async.commit_group;\n" ::: "memory"); }
-template <int N>
-__device__ __forceinline__ void cp_async_wait() {
-  asm volatile("cp.async.wait_group %0;\n" ::"n"(N) : "memory");
+__device__ __forceinline__ void mbar_init(unsigned bar, unsigned count) {
+  asm volatile("mbarrier.init.shared::cta.b64 [%0], %1;\n" ::"r"(bar), "r"(count) : "memory");
 }
+__device__ __forceinline__ void mbar_expect_tx(unsigned bar, unsigned bytes) {
+  asm volatile("mbarrier.arrive.expect_tx.shared::cta.b64 _, [%0], %1;\n" ::"r"(bar), "r"(bytes) : "memory");
+}
+__device__ __forceinline__ bool mbar_try_wait(unsigned bar, unsigned parity) {
+  unsigned ok;
+  asm volatile(
+      "{\n .reg .pred p;\n mbarrier.try_wait.parity.shared::cta.b64 p, [%1], %2;\n selp.u32 %0, 1, 0, p;\n}\n"
+      : "=r"(ok)
+      : "r"(bar), "r"(parity)
+      : "memory");
+  return ok != 0;
+}
+// Bounded wait for the phase with this parity; false if the bound ran out.
+__device__ __forceinline__ bool mbar_wait(unsigned bar, unsigned parity) {
+  for (unsigned s = 0; s < kWaitSpins; ++s)
+    if (mbar_try_wait(bar, parity)) return true;
+  return false;
+}
+__device__ __forceinline__ void bulk_g2s(unsigned dst, const void* src, unsigned bytes, unsigned bar) {
+  asm volatile(
+      "cp.async.bulk.shared::cluster.global.mbarrier::complete_tx::bytes [%0], [%1], %2, [%3];\n" ::"r"(dst),
+      "l"(src), "r"(bytes), "r"(bar)
+      : "memory");
+}
+__device__ __forceinline__ void fence_proxy_async() { asm volatile("fence.proxy.async.shared::cta;\n" ::: "memory"); }
 
-// One lane's C columns of row p (p points at the lane's first column), from
-// global (__ldg) or shared memory.
+// One lane's C columns of row p (p points at the lane's first column).
 template <class T, int C, bool GLOBAL>
 __device__ __forceinline__ void load_v(const T* p, typename UK<T, C>::V (&v)[UK<T, C>::NV]) {
   if constexpr (sizeof(T) == 4 && C == 4) {
@@ -341,38 +369,38 @@ __device__ __forceinline__ void zero_val(T& a) {
 }
 __device__ __forceinline__ void zero_val(float2& a) { a = make_float2(0.f, 0.f); }
 
-// Exclusive scan of popc(mask) over the 32 records of a batch; total in `tot`.
+template <class T, int C>
+constexpr size_t band_smem_bytes() {
+  return (size_t)kWarpsUT * sizeof(WarpSmem<T, C>);
+}
+
+// Exclusive scan of popc(mask) over lanes 0..kBatch-1 (the batch's records);
+// the batch's pair count in `tot`.
 __device__ __forceinline__ int batch_scan(uint32_t rec, int lane, int& tot) {
   const int pc = __popc(rec & 0xffu);
   int incl = pc;
 #pragma unroll
-  for (int o = 1; o < 32; o <<= 1) {
+  for (int o = 1; o < kBatch; o <<= 1) {
     const int y = __shfl_up_sync(0xffffffffu, incl, o);
     if (lane >= o) incl += y;
   }
-  tot = __shfl_sync(0xffffffffu, incl, 31);
+  tot = __shfl_sync(0xffffffffu, incl, kBatch - 1);
   return incl - pc;
 }
 
-template <class T, int C, int kRing>
-constexpr size_t band_smem_bytes() {
-  return (size_t)kWarpsUT * kRing * sizeof(RingStage<T, C>);
-}
-
-template <class T, int C, int kRing>
+template <class T, int C>
 __global__ void __launch_bounds__(kWarpsUT * 32, UK<T, C>::MINB)
-k_spmm_band(int64_t n_atoms, const int64_t* __restrict__ uptr, const int64_t* __restrict__ pptr,
+k_spmm_band(int n_atoms, const int64_t* __restrict__ uptr, const int64_t* __restrict__ pptr,
             const uint32_t* __restrict__ urec, const void* __restrict__ pw, const T* __restrict__ diag,
             const T* __restrict__ X, int64_t ldx, T* Y, int64_t ldy, const T* Yin, int64_t ldyin,
             T* __restrict__ Acc, int64_t ldacc, int c0, int ncols, EpiT ep, const double* __restrict__ Q,
             int64_t ndof, const double* __restrict__ coef) {
   using V = typename UK<T, C>::V;
-  using St = RingStage<T, C>;
   constexpr int NV = UK<T, C>::NV;
   constexpr int P = 32 * C;
-  constexpr int XB = C * (int)sizeof(T);          // bytes of one lane's slice of one row
-  constexpr int WB = (int)sizeof(WRaw<T>);         // bytes of one pair's w
-  extern __shared__ __align__(16) unsigned char band_smem[];
+  constexpr int WB = (int)sizeof(WRaw<T>);
+  constexpr int VEC = 16 / (int)sizeof(T);            // elements per 16 bytes
+  extern __shared__ __align__(128) unsigned char band_smem[];
   __shared__ double s_coef[8 * P];
   if (ep.r > 0) {
     for (int t = threadIdx.x; t < ep.r * P; t += kWarpsUT * 32) s_coef[t] = coef[t];
@@ -380,12 +408,24 @@ k_spmm_band(int64_t n_atoms, const int64_t* __restrict__ uptr, const int64_t* __
   }
   const int lane = threadIdx.x & 31;
   const int warp = threadIdx.x >> 5;
-  St* ring = reinterpret_cast<St*>(band_smem) + warp * kRing;
+  WarpSmem<T, C>* sm = reinterpret_cast<WarpSmem<T, C>*>(band_smem) + warp;
+  const unsigned bar0 = smem_u32(&sm->bar[0]), bar1 = smem_u32(&sm->bar[1]);
+  if (lane == 0) {
+    mbar_init(bar0, 1);
+    mbar_init(bar1, 1);
+  }
+  fence_proxy_async();
+  __syncwarp();
+  unsigned ph0 = 0u, ph1 = 0u;               // parity of the next phase to complete, per buffer
+  bool pend0 = false, pend1 = false;         // a staged batch not yet waited for, per buffer
   const bool on = lane * C < ncols;          // lane inside the panel
-  const T* Xc = X + c0 + lane * C;
+  // bytes of one staged row segment: the panel's columns rounded up to 16 bytes
+  // (the rounding stays inside the row: leading dimensions are multiples of VEC)
+  const unsigned row_bytes = (unsigned)(((ncols + VEC - 1) / VEC) * VEC * (int)sizeof(T));
+  const T* Xp = X + c0;
   const unsigned char* pwb = static_cast<const unsigned char*>(pw);
-  const int64_t ntiles = (n_atoms + kTile - 1) / kTile;
-  for (int64_t t = (int64_t)blockIdx.x * kWarpsUT + warp; t < ntiles; t += (int64_t)gridDim.x * kWarpsUT) {
+  const int ntiles = (n_atoms + kTile - 1) / kTile;
+  for (int t = blockIdx.x * kWarpsUT + warp; t < ntiles; t += gridDim.x * kWarpsUT) {
     V acc[kTile][3][NV];
 #pragma unroll
     for (int r = 0; r < kTile; ++r)
@@ -393,77 +433,99 @@ k_spmm_band(int64_t n_atoms, const int64_t* __restrict__ uptr, const int64_t* __
       for (int a = 0; a < 3; ++a)
 #pragma unroll
         for (int k = 0; k < NV; ++k) zero_val(acc[r][a][k]);
-    const int64_t u0 = uptr[t], u1 = uptr[t + 1];
-    // batch at ub (rec, excl, tot) and the next one (recn, excln, totn)
-    int64_t ub = u0;
-    int64_t pbase = pptr[t];
-    uint32_t rec = (u0 + lane < u1) ? __ldg(urec + u0 + lane) : 0u;
-    int tot;
-    int excl = batch_scan(rec, lane, tot);
-    uint32_t recn = (u0 + kUB + lane < u1) ? __ldg(urec + u0 + kUB + lane) : 0u;
-    int totn;
-    int excln = batch_scan(recn, lane, totn);
-    // stage union gg (gg - ub < 2 * kUB) into its ring slot
-    auto issue = [&](int64_t gg) {
-      if (gg < u1) {
-        const int li = (int)(gg - ub);
-        uint32_t rr;
-        int64_t q;
-        if (li < kUB) {
-          rr = __shfl_sync(0xffffffffu, rec, li);
-          q = pbase + __shfl_sync(0xffffffffu, excl, li);
-        } else {
-          rr = __shfl_sync(0xffffffffu, recn, li - kUB);
-          q = pbase + tot + __shfl_sync(0xffffffffu, excln, li - kUB);
-        }
-        St* st = ring + ((gg - u0) & (kRing - 1));
-        if (on) {
-          const T* p = Xc + 3 * (int64_t)(rr >> 8) * ldx;
-          cp_async<XB>(&st->x[0][lane * C], p);
-          cp_async<XB>(&st->x[1][lane * C], p + ldx);
-          cp_async<XB>(&st->x[2][lane * C], p + 2 * ldx);
-        }
-        if (lane < __popc(rr & 0xffu)) {
-          const unsigned char* src = pwb + (q + lane) * WB;
-          unsigned char* dst = reinterpret_cast<unsigned char*>(&st->w[lane]);
-#pragma unroll
-          for (int o = 0; o < WB; o += 16) cp_async<16>(dst + o, src + o);
-        }
-      }
-      cp_async_commit();
+    const int64_t ubase = uptr[t];
+    const int nu = (int)(uptr[t + 1] - ubase);
+    const int64_t pbase = pptr[t];
+    const int nb = (nu + kBatch - 1) / kBatch;
+    // records of the batch being multiplied (rc), being staged next (rs) and the
+    // one after it (rp), in lanes 0..kBatch-1; ec: their exclusive pair offsets
+    auto rec_of = [&](int bb) -> uint32_t {
+      const int u = bb * kBatch + lane;
+      return (lane < kBatch && u < nu) ? __ldg(urec + ubase + u) : 0u;
     };
-#pragma unroll
-    for (int s = 0; s < kRing - 1; ++s) issue(u0 + s);
-    for (int64_t g = u0; g < u1; ++g) {
-      if (g - ub == kUB) {              // next batch of records
-        ub += kUB;
-        pbase += tot;
-        rec = recn;
-        excl = excln;
-        tot = totn;
-        recn = (ub + kUB + lane < u1) ? __ldg(urec + ub + kUB + lane) : 0u;
-        excln = batch_scan(recn, lane, totn);
+    int qstage = 0;                          // tile-relative first pair of the next batch to stage
+    // stage batch bb (records r) into buffer bb & 1; returns the exclusive offsets
+    auto issue = [&](int bb, uint32_t r) -> int {
+      const int s = bb & 1;
+      int tot;
+      const int ex = batch_scan(r, lane, tot);
+      const int cnt = (nu - bb * kBatch) < kBatch ? (nu - bb * kBatch) : kBatch;
+      Batch<T, C>* B = &sm->buf[s];
+      const unsigned bar = s ? bar1 : bar0;
+      if (lane == 0) mbar_expect_tx(bar, (unsigned)cnt * 3u * row_bytes + (unsigned)tot * WB);
+      __syncwarp();
+      if (lane < cnt) {
+        const T* p = Xp + (int64_t)(3 * (int)(r >> 8)) * ldx;
+        bulk_g2s(smem_u32(&B->x[lane][0][0]), p, row_bytes, bar);
+        bulk_g2s(smem_u32(&B->x[lane][1][0]), p + ldx, row_bytes, bar);
+        bulk_g2s(smem_u32(&B->x[lane][2][0]), p + 2 * ldx, row_bytes, bar);
       }
-      __syncwarp();                     // every lane is done with the slot issue() refills
-      issue(g + kRing - 1);
-      cp_async_wait<kRing - 1>();       // this lane's copies of union g have landed
-      __syncwarp();                     // ... and every other lane's (the w values)
-      const St* st = ring + ((g - u0) & (kRing - 1));
-      const unsigned m = __shfl_sync(0xffffffffu, rec, (int)(g - ub)) & 0xffu;
-      V x[3][NV];
-      load_v<T, C, false>(&st->x[0][lane * C], x[0]);
-      load_v<T, C, false>(&st->x[1][lane * C], x[1]);
-      load_v<T, C, false>(&st->x[2][lane * C], x[2]);
-      nib_dispatch<0, T, V, NV>(m & 15u, acc, x, st->w);
-      nib_dispatch<4, T, V, NV>(m >> 4, acc, x, st->w + __popc(m & 15u));
+      if (lane == kBatch && tot > 0)
+        bulk_g2s(smem_u32(&B->w[0]), pwb + (pbase + qstage) * WB, (unsigned)tot * WB, bar);
+      qstage += tot;
+      if (s)
+        pend1 = true;
+      else
+        pend0 = true;
+      return ex;
+    };
+    uint32_t rc = rec_of(0), rs = rec_of(1), rp = 0u;
+    int ec = 0, es = 0;
+    __syncwarp();                            // the previous tile's reads of both buffers are done
+    fence_proxy_async();
+    if (nb > 0) ec = issue(0, rc);
+    bool ok = true;
+    for (int bb = 0; bb < nb; ++bb) {
+      if (bb + 1 < nb) {
+        rp = rec_of(bb + 2);
+        __syncwarp();                        // every lane is done reading the buffer issue() refills
+        fence_proxy_async();
+        es = issue(bb + 1, rs);
+      }
+      const int s = bb & 1;
+      if (!mbar_wait(s ? bar1 : bar0, s ? ph1 : ph0)) {
+        ok = false;
+        break;
+      }
+      if (s) {
+        ph1 ^= 1u;
+        pend1 = false;
+      } else {
+        ph0 ^= 1u;
+        pend0 = false;
+      }
+      const Batch<T, C>* B = &sm->buf[s];
+      const int cnt = (nu - bb * kBatch) < kBatch ? (nu - bb * kBatch) : kBatch;
+      for (int k = 0; k < cnt; ++k) {
+        const unsigned m = __shfl_sync(0xffffffffu, rc, k) & 0xffu;
+        const int qk = __shfl_sync(0xffffffffu, ec, k);
+        V x[3][NV];
+        load_v<T, C, false>(&B->x[k][0][lane * C], x[0]);
+        load_v<T, C, false>(&B->x[k][1][lane * C], x[1]);
+        load_v<T, C, false>(&B->x[k][2][lane * C], x[2]);
+        const WRaw<T>* sw = B->w + qk;
+        nib_dispatch<0, T, V, NV>(m & 15u, acc, x, sw);
+        nib_dispatch<4, T, V, NV>(m >> 4, acc, x, sw + __popc(m & 15u));
+      }
+      rc = rs;
+      ec = es;
+      rs = rp;
+    }
+    if (!ok) {
+      // a wait ran out: record it, let this warp's outstanding copies land (again
+      // bounded), and stop
+      if (lane == 0) atomicExch(&g_band_status, kBandTimeout);
+      if (pend0) mbar_wait(bar0, ph0);
+      if (pend1) mbar_wait(bar1, ph1);
+      return;
     }
     // epilogue: (H X)_i = D_i X_i - S_i, then the fused combination per element
+    if (!on) continue;
 #pragma unroll
     for (int r = 0; r < kTile; ++r) {
-      const int64_t i = t * kTile + r;
+      const int i = t * kTile + r;
       if (i >= n_atoms) break;
-      if (!on) continue;
-      const T* d = diag + 8 * i;
+      const T* d = diag + 8 * (int64_t)i;
       const T dxx = d[0], dyy = d[1], dzz = d[2], dxy = d[3], dxz = d[4], dyz = d[5];
       double al = ep.alpha, ga = ep.gamma, be = ep.beta;
       if (ep.seg_coef != nullptr) {
@@ -472,15 +534,17 @@ k_spmm_band(int64_t n_atoms, const int64_t* __restrict__ uptr, const int64_t* __
         ga = __ldg(ep.seg_coef + 3 * sg + 1);
         be = __ldg(ep.seg_coef + 3 * sg + 2);
       }
-      const int64_t r0 = 3 * i;
+      const int64_t r0 = 3 * (int64_t)i;
+      const T* xr = Xp + r0 * ldx + lane * C;
       T x0[C], x1[C], x2[C];
-      load_s<T, C>(Xc + r0 * ldx, x0);
-      load_s<T, C>(Xc + (r0 + 1) * ldx, x1);
-      load_s<T, C>(Xc + (r0 + 2) * ldx, x2);
+      load_s<T, C>(xr, x0);
+      load_s<T, C>(xr + ldx, x1);
+      load_s<T, C>(xr + 2 * ldx, x2);
       T s0[C], s1[C], s2[C];
       to_scalars<T, C>(acc[r][0], s0);
       to_scalars<T, C>(acc[r][1], s1);
       to_scalars<T, C>(acc[r][2], s2);
+      const T alf = (T)al, gaf = (T)ga, bef = (T)be;
 #pragma unroll
       for (int a = 0; a < 3; ++a) {
         const int64_t row = r0 + a;
@@ -492,10 +556,14 @@ k_spmm_band(int64_t n_atoms, const int64_t* __restrict__ uptr, const int64_t* __
                       : (a == 1) ? (dxy * x0[c] + dyy * x1[c] + dyz * x2[c]) - s1[c]
                                  : (dxz * x0[c] + dyz * x1[c] + dzz * x2[c]) - s2[c];
           const T xa_ = (a == 0) ? x0[c] : (a == 1) ? x1[c] : x2[c];
-          double y = al * (double)h + ga * (double)xa_;
-          if (ep.has_yin) y += be * (double)yin[c];
-          for (int q = 0; q < ep.r; ++q) y += Q[q * ndof + row] * s_coef[q * P + lane * C + c];
-          yv[c] = (T)y;
+          T y = alf * h + gaf * xa_;
+          if (ep.has_yin) y += bef * yin[c];
+          if (ep.r > 0) {
+            double yq = (double)y;
+            for (int q = 0; q < ep.r; ++q) yq += Q[q * ndof + row] * s_coef[q * P + lane * C + c];
+            y = (T)yq;
+          }
+          yv[c] = y;
         }
         store_s<T, C>(Y + row * ldy + c0 + lane * C, yv);
         if (ep.accumulate) {
@@ -508,7 +576,6 @@ k_spmm_band(int64_t n_atoms, const int64_t* __restrict__ uptr, const int64_t* __
       }
     }
   }
-  cp_async_wait<0>();   // nothing of this warp's may still be in flight at exit
 }
 
 constexpr int kThreads = 256;
@@ -555,21 +622,19 @@ k_qx_final_t(const double* __restrict__ partial, int nblk, int r, int P, double 
 
 constexpr int kQxBlocksT = 296;
 
-// Process-wide launch choices (autotuner hooks): the widest FP32 panel (128 or
-// 64 columns) and the ring depth (4, 8 or 16 union columns per warp).
+// Process-wide launch choice (autotuner hook): the widest FP32 panel, 128 or 64.
 std::atomic<int> g_band_panel32{128};
-std::atomic<int> g_band_ring{kRingDefault};
 
 // Grid of the band kernel: its resident blocks per SM (registers and the ring's
 // dynamic shared memory, opted in once per instantiation) times the SM count.
-template <class T, int C, int R>
+template <class T, int C>
 int band_grid(int64_t ntiles) {
   static int per_sm = 0;
   if (per_sm == 0) {
     int nb = 0;
-    const size_t sm = band_smem_bytes<T, C, R>();
-    cudaFuncSetAttribute(k_spmm_band<T, C, R>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sm);
-    if (cudaOccupancyMaxActiveBlocksPerMultiprocessor(&nb, k_spmm_band<T, C, R>, kWarpsUT * 32, sm) != cudaSuccess ||
+    const size_t sm = band_smem_bytes<T, C>();
+    cudaFuncSetAttribute(k_spmm_band<T, C>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sm);
+    if (cudaOccupancyMaxActiveBlocksPerMultiprocessor(&nb, k_spmm_band<T, C>, kWarpsUT * 32, sm) != cudaSuccess ||
         nb < 1)
       nb = 1;
     per_sm = nb;
@@ -593,32 +658,21 @@ cudaError_t band_launch(int64_t n, const int64_t* uptr, const int64_t* pptr, con
                                                                                    hot_shift, coef);
   }
   const int64_t ntiles = (n + kTile - 1) / kTile;
-#define INCH_BAND(R)                                                                                       \
-  k_spmm_band<T, C, R><<<band_grid<T, C, R>(ntiles), kWarpsUT * 32, band_smem_bytes<T, C, R>(), s>>>(        \
-      n, uptr, pptr, urec, pw, diag, X, ldx, Y, ldy, Yin, ldyin, Acc, ldacc, c0, ncols, ep, Q, ndof, coef);
-  const int ring = g_band_ring.load();
-  if (ring == 4) {
-    INCH_BAND(4)
-  } else if (ring == 16) {
-    INCH_BAND(16)
-  } else {
-    INCH_BAND(8)
-  }
-#undef INCH_BAND
+k_spmm_band<T, C><<<band_grid<T, C>(ntiles), kWarpsUT * 32, band_smem_bytes<T, C>(), s>>>(
+      (int)n, uptr, pptr, urec, pw, diag, X, ldx, Y, ldy, Yin, ldyin, Acc, ldacc, c0, ncols, ep, Q, ndof, coef);
   return cudaGetLastError();
 }
 
 
 
-// Whether every vector operand allows loads/stores of `elems` elements per lane.
-template <class T>
-bool band_aligned(int elems, const T* X, int64_t ldx, const T* Y, int64_t ldy, const T* Yin, int64_t ldyin,
-                  const T* Acc, int64_t ldacc, int c0) {
-  const uintptr_t al = (uintptr_t)elems * sizeof(T);
-  bool ok = (ldx % elems == 0) && (ldy % elems == 0) && (c0 % elems == 0) && ((uintptr_t)X % al == 0) &&
-            ((uintptr_t)Y % al == 0);
-  if (Yin) ok = ok && (ldyin % elems == 0) && ((uintptr_t)Yin % al == 0);
-  if (Acc) ok = ok && (ldacc % elems == 0) && ((uintptr_t)Acc % al == 0);
+// Whether every vector block starts on 16 bytes with a leading dimension that is a
+// multiple of vec elements (the bulk copies and vector stores of the band kernel).
+inline bool band_vectors_aligned(int vec, int esize, const void* X, int64_t ldx, const void* Y, int64_t ldy,
+                                 const void* Yin, int64_t ldyin, const void* Acc, int64_t ldacc) {
+  (void)esize;
+  bool ok = (ldx % vec == 0) && (ldy % vec == 0) && ((uintptr_t)X % 16 == 0) && ((uintptr_t)Y % 16 == 0);
+  if (Yin) ok = ok && (ldyin % vec == 0) && ((uintptr_t)Yin % 16 == 0);
+  if (Acc) ok = ok && (ldacc % vec == 0) && ((uintptr_t)Acc % 16 == 0);
   return ok;
 }
 
@@ -629,37 +683,27 @@ cudaError_t band_run(int64_t n, const int64_t* uptr, const int64_t* pptr, const 
                      double* coef, cudaStream_t s) {
   cudaError_t err = cudaSuccess;
   int c0 = 0;
-  const T* Yin_ = ep.has_yin ? Yin : nullptr;
-  T* Acc_ = ep.accumulate ? Acc : nullptr;
   while (c0 < b && err == cudaSuccess) {
     const int rem = b - c0;
+    bool wide = false;
     if constexpr (sizeof(T) == 4) {
-      const int widest = g_band_panel32.load();
-      if (widest >= 128 && rem >= 128 && band_aligned<T>(4, X, ldx, Y, ldy, Yin_, ldyin, Acc_, ldacc, c0)) {
+      if (g_band_panel32.load() >= 128 && rem >= 128) {
         err = band_launch<T, 4>(n, uptr, pptr, urec, pw, diag, X, ldx, Y, ldy, Yin, ldyin, Acc, ldacc, c0, 128, ep,
                                 Q, hot_shift, partial, coef, s);
         c0 += 128;
-      } else if (rem >= 64 && band_aligned<T>(2, X, ldx, Y, ldy, Yin_, ldyin, Acc_, ldacc, c0)) {
-        err = band_launch<T, 2>(n, uptr, pptr, urec, pw, diag, X, ldx, Y, ldy, Yin, ldyin, Acc, ldacc, c0, 64, ep,
-                                Q, hot_shift, partial, coef, s);
-        c0 += 64;
-      } else {
-        const int nc = rem < 32 ? rem : 32;
-        err = band_launch<T, 1>(n, uptr, pptr, urec, pw, diag, X, ldx, Y, ldy, Yin, ldyin, Acc, ldacc, c0, nc, ep,
-                                Q, hot_shift, partial, coef, s);
-        c0 += nc;
+        wide = true;
       }
+    }
+    if (wide) {
+    } else if (rem >= 64) {
+      err = band_launch<T, 2>(n, uptr, pptr, urec, pw, diag, X, ldx, Y, ldy, Yin, ldyin, Acc, ldacc, c0, 64, ep, Q,
+                              hot_shift, partial, coef, s);
+      c0 += 64;
     } else {
-      if (rem >= 64 && band_aligned<T>(2, X, ldx, Y, ldy, Yin_, ldyin, Acc_, ldacc, c0)) {
-        err = band_launch<T, 2>(n, uptr, pptr, urec, pw, diag, X, ldx, Y, ldy, Yin, ldyin, Acc, ldacc, c0, 64, ep,
-                                Q, hot_shift, partial, coef, s);
-        c0 += 64;
-      } else {
-        const int nc = rem < 32 ? rem : 32;
-        err = band_launch<T, 1>(n, uptr, pptr, urec, pw, diag, X, ldx, Y, ldy, Yin, ldyin, Acc, ldacc, c0, nc, ep,
-                                Q, hot_shift, partial, coef, s);
-        c0 += nc;
-      }
+      const int nc = rem < 32 ? rem : 32;
+      err = band_launch<T, 1>(n, uptr, pptr, urec, pw, diag, X, ldx, Y, ldy, Yin, ldyin, Acc, ldacc, c0, nc, ep, Q,
+                              hot_shift, partial, coef, s);
+      c0 += nc;
     }
   }
   return err;
@@ -734,16 +778,21 @@ extern "C" size_t inch_spmm_tiles_workspace_size(void) {
   return s.bytes();
 }
 
-extern "C" inch_status inch_spmm_band_tune(int32_t widest_fp32_panel, int32_t ring_depth) {
+extern "C" inch_status inch_spmm_band_tune(int32_t widest_fp32_panel) {
   INCH_REQUIRE(widest_fp32_panel == 64 || widest_fp32_panel == 128, INCH_INVALID_ARG,
                "inch_spmm_band_tune: widest FP32 panel must be 64 or 128");
-  INCH_REQUIRE(ring_depth == 4 || ring_depth == 8 || ring_depth == 16, INCH_INVALID_ARG,
-               "inch_spmm_band_tune: ring depth must be 4, 8 or 16");
   g_band_panel32.store(widest_fp32_panel);
-  g_band_ring.store(ring_depth);
   return INCH_OK;
 }
 
+extern "C" inch_status inch_spmm_band_status(int32_t* status_host) {
+  INCH_REQUIRE(status_host != nullptr, INCH_INVALID_ARG, "inch_spmm_band_status: NULL argument");
+  int v = 0, zero = 0;
+  INCH_CUDA(cudaMemcpyFromSymbol(&v, g_band_status, sizeof(int)));
+  INCH_CUDA(cudaMemcpyToSymbol(g_band_status, &zero, sizeof(int)));
+  *status_host = v;
+  return INCH_OK;
+}
 extern "C" inch_status inch_spmm_tiles(int32_t prec, int64_t n, const int64_t* tile_uptr, const int64_t* tile_pptr,
                                        const uint32_t* urec, const void* pw, const void* diag, const void* Xv,
                                        int64_t ldx, int32_t b, void* Yv, int64_t ldy, const void* Yinv, int64_t ldyin,
@@ -761,6 +810,11 @@ extern "C" inch_status inch_spmm_tiles(int32_t prec, int64_t n, const int64_t* t
   INCH_REQUIRE(!e.accumulate || (Accv && ldacc >= b), INCH_INVALID_ARG, "inch_spmm_tiles: accumulate needs Acc");
   INCH_REQUIRE(((uintptr_t)pw & 15) == 0 && ((uintptr_t)diag & 15) == 0, INCH_INVALID_ARG,
                "inch_spmm_tiles: store buffers must be 16-byte aligned");
+  const int vec = prec == 32 ? 4 : 2;
+  INCH_REQUIRE(band_vectors_aligned(vec, prec == 32 ? 4 : 8, Xv, ldx, Yv, ldy, e.beta != 0.0 ? Yinv : nullptr, ldyin,
+                                    e.accumulate ? Accv : nullptr, ldacc),
+               INCH_INVALID_ARG,
+               "inch_spmm_tiles: vector blocks must start on 16 bytes with leading dimensions multiples of %d", vec);
   double *partial = nullptr, *coef = nullptr;
   if (e.r > 0) {
     Carver c(ws, ws_bytes);
@@ -799,6 +853,11 @@ extern "C" inch_status inch_spmm_tiles_seg(int32_t prec, int64_t n, const int64_
   INCH_REQUIRE(Yinv == nullptr || ldyin >= b, INCH_INVALID_ARG, "inch_spmm_tiles_seg: ldyin below b");
   INCH_REQUIRE(((uintptr_t)pw & 15) == 0 && ((uintptr_t)diag & 15) == 0, INCH_INVALID_ARG,
                "inch_spmm_tiles_seg: store buffers must be 16-byte aligned");
+  const int vec = prec == 32 ? 4 : 2;
+  INCH_REQUIRE(band_vectors_aligned(vec, prec == 32 ? 4 : 8, Xv, ldx, Yv, ldy, Yinv, ldyin, nullptr, 0),
+               INCH_INVALID_ARG,
+               "inch_spmm_tiles_seg: vector blocks must start on 16 bytes with leading dimensions multiples of %d",
+               vec);
   EpiT ep{0.0, 0.0, 0.0, 0.0, 0, 0, Yinv != nullptr ? 1 : 0, seg_coef, atom_seg};
   cudaError_t err;
   if (prec == 32)

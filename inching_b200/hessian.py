@@ -186,12 +186,27 @@ class HessianStore:
         if self._tiled(prec, b):
             t = self.tiles
             pw = t["pw64"] if prec == 64 else t["pw32"]
-            if X.dim() == 1:
-                kw = {k: (v[:, None] if (k in ("Yin", "acc") and v is not None) else v) for k, v in epilogue.items()}
-                _native.spmm_tiles(prec, self.n_atoms, t["uptr"], t["pptr"], t["urec"], pw, diag, X[:, None],
-                                   out[:, None], **kw)
+            vec = 4 if prec == 32 else 2
+            X2 = X[:, None] if X.dim() == 1 else X
+            out2 = out[:, None] if out.dim() == 1 else out
+            kw = {k: (v[:, None] if (k in ("Yin", "acc") and v is not None and v.dim() == 1) else v)
+                  for k, v in epilogue.items()}
+            blocks = [X2, out2] + [kw[k] for k in ("Yin", "acc") if kw.get(k) is not None]
+            if all(_band_aligned(m, vec) for m in blocks):
+                _native.spmm_tiles(prec, self.n_atoms, t["uptr"], t["pptr"], t["urec"], pw, diag, X2, out2, **kw)
                 return out
-            _native.spmm_tiles(prec, self.n_atoms, t["uptr"], t["pptr"], t["urec"], pw, diag, X, out, **epilogue)
+            # the band kernel stages 16-byte rows: run on padded copies of the blocks
+            bp = (b + vec - 1) // vec * vec
+            pad = lambda m: torch.nn.functional.pad(m, (0, bp - b)).contiguous()
+            kwp = dict(kw)
+            for k in ("Yin", "acc"):
+                if kw.get(k) is not None:
+                    kwp[k] = pad(kw[k])
+            outp = torch.empty((X2.shape[0], bp), dtype=X2.dtype, device=X2.device)
+            _native.spmm_tiles(prec, self.n_atoms, t["uptr"], t["pptr"], t["urec"], pw, diag, pad(X2), outp, **kwp)
+            out2.copy_(outp[:, :b])
+            if kw.get("acc") is not None:
+                kw["acc"].copy_(kwp["acc"][:, :b])
             return out
         if X.dim() == 1 or X.shape[1] <= 64:
             return _native.spmm(prec, self.n_atoms, self.rowptr, ent, diag, X, out, **epilogue)
@@ -209,7 +224,8 @@ class HessianStore:
         """out = alpha_s (H X) + gamma_s X + beta_s Yin with per-segment coefficients
         (block-diagonal stores of many structures; pair layout)."""
         ent, diag = self.store(prec)
-        if self._tiled(prec, X.shape[1]):
+        vec = 4 if prec == 32 else 2
+        if self._tiled(prec, X.shape[1]) and all(_band_aligned(m, vec) for m in (X, out, Yin) if m is not None):
             t = self.tiles
             pw = t["pw64"] if prec == 64 else t["pw32"]
             return _native.spmm_tiles_seg(prec, self.n_atoms, t["uptr"], t["pptr"], t["urec"], pw, diag, X, out,
@@ -252,6 +268,12 @@ class HessianStore:
         A = sp.csr_matrix((V[keep], (R[keep], C[keep])), shape=self.shape)
         A.sum_duplicates()
         return A
+
+
+def _band_aligned(m, vec):
+    """Whether a (rows, b) block can go to the band kernel as it is: its data starts
+    on 16 bytes and its leading dimension is a multiple of vec elements."""
+    return m.data_ptr() % 16 == 0 and m.stride(1) == 1 and m.stride(0) % vec == 0
 
 
 def _launches(b, prec):

@@ -354,13 +354,15 @@ inch_status inch_tile_store_fill(const double* X_dev, int64_t n_atoms, double rc
 size_t inch_spmm_tiles_workspace_size(void);
 /* The band-tile product: one warp per 8-row tile and column panel (FP32 panels of
  * 128 columns with the packed f32x2 FMAs of sm_100, or 64 / 32; FP64 panels of
- * 64 / 32), each union column's X_j gathered once for all rows of its mask.
- * Any b >= 1 (the library walks the panels; b < 32 runs one partial panel).
- * Replaces the same two cuSPARSE SpMVs as inch_spmm (Burn/Krylov/T3.py:138-156),
- * with the same fused epilogue.  Vector rows whose leading dimensions and column
- * offset are multiples of 4 (FP32) or 2 elements take the vector panels; any
- * other alignment runs scalar panels.  ws: inch_spmm_tiles_workspace_size()
- * bytes, used only when ep->r > 0. */
+ * 64 / 32), each union column's X_j staged once by the bulk-copy (TMA) engine
+ * and applied to all rows of its mask.  Any b >= 1 (the library walks the
+ * panels; the last one may be partial).  Replaces the same two cuSPARSE SpMVs as
+ * inch_spmm (Burn/Krylov/T3.py:138-156), with the same fused epilogue.  Every
+ * vector block (X, Y, Yin, Acc) must start on 16 bytes and have a leading
+ * dimension that is a multiple of 4 (FP32) or 2 (FP64) elements, else
+ * INCH_INVALID_ARG; rows of X are read up to the next 16-byte boundary past the
+ * last column, which the leading dimension keeps inside the row.  ws: inch_spmm_tiles_workspace_size() bytes, used only when
+ * ep->r > 0. */
 inch_status inch_spmm_tiles(int32_t prec, int64_t n_atoms, const int64_t* tile_uptr_dev,
                             const int64_t* tile_pptr_dev, const uint32_t* urec_dev, const void* pw_dev,
                             const void* diag_dev, const void* X_dev, int64_t ldx, int32_t b,
@@ -375,10 +377,14 @@ inch_status inch_spmm_tiles_seg(int32_t prec, int64_t n_atoms, const int64_t* ti
                                 const void* diag_dev, const void* X_dev, int64_t ldx, int32_t b,
                                 void* Y_dev, int64_t ldy, const void* Yin_dev, int64_t ldyin,
                                 const int32_t* atom_seg_dev, const double* seg_coef_dev, cudaStream_t stream);
-/* Launch choices of the band-tile product for this process: the widest FP32
- * panel (128 or 64 columns) and the depth of each warp's staging ring (4, 8 or
- * 16 union columns in flight).  The autotuner's hook (no reference counterpart). */
-inch_status inch_spmm_band_tune(int32_t widest_fp32_panel, int32_t ring_depth);
+/* Widest FP32 panel of the band-tile product for this process (128 or 64
+ * columns): the autotuner's hook (no reference counterpart). */
+inch_status inch_spmm_band_tune(int32_t widest_fp32_panel);
+/* Status word of the band-tile kernels (synchronises): 0, or 1 if a bounded
+ * wait for a staged batch ran out in some launch since the last call (the
+ * affected launch stopped early; its output is incomplete).  Reading clears it.
+ * No reference counterpart. */
+inch_status inch_spmm_band_status(int32_t* status_host);
 
 /* Allocation-free form of inch_spmm (no counterpart in the reference).  For
  * callers that cannot provide device scratch -- hosts running on another
