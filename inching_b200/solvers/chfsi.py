@@ -533,21 +533,26 @@ def chfsi_lean(A, k, tol=1e-6, Q=None, precision="mixed", degree=None, guard=Non
         G = torch.zeros((act_n, act_n), dtype=torch.float64, device=dev)
         for cs in range(L, p, chunk):
             ce = min(cs + chunk, p)
-            HYc = A.matmul(B[:, cs:ce].contiguous(), prec=64)
-            G[:, cs - L:ce - L] = B[:, L:].t() @ HYc
+            with ph("rr_spmm"):
+                HYc = A.matmul(B[:, cs:ce].contiguous(), prec=64)
+            with ph("rr_gram"):
+                G[:, cs - L:ce - L] = B[:, L:].t() @ HYc
             del HYc
         G = 0.5 * (G + G.t())
-        th, Wd = eigh_sym(G)
-        for rs in _rows(n, row_chunk):
-            B[rs, L:] = B[rs, L:] @ Wd
+        with ph("rr_eigh"):
+            th, Wd = eigh_sym(G)
+        with ph("rr_rotate"):
+            for rs in _rows(n, row_chunk):
+                B[rs, L:] = B[rs, L:] @ Wd
         res = np.full(len(th), np.inf)
         last = min(len(th), k - L, window)
         thd = torch.from_numpy(th[:last].copy()).to(dev)
-        for cs in range(0, last, chunk):
-            ce = min(cs + chunk, last)
-            Yc = B[:, L + cs:L + ce].contiguous()
-            R = A.matmul(Yc, prec=64) - Yc * thd[cs:ce][None, :]
-            res[cs:ce] = torch.linalg.vector_norm(R, dim=0).cpu().numpy()
+        with ph("rr_residual"):
+            for cs in range(0, last, chunk):
+                ce = min(cs + chunk, last)
+                Yc = B[:, L + cs:L + ce].contiguous()
+                R = A.matmul(Yc, prec=64) - Yc * thd[cs:ce][None, :]
+                res[cs:ce] = torch.linalg.vector_norm(R, dim=0).cpu().numpy()
         return th, res
 
     ph = _Phases(profile)
@@ -602,6 +607,8 @@ def chfsi_lean(A, k, tol=1e-6, Q=None, precision="mixed", degree=None, guard=Non
             th, res = rayleigh_ritz(L)
     converged = L >= k
     # final FP64 Rayleigh-Ritz over the first k columns, explicit residuals
+    ph_final = ph("final_f64")
+    ph_final.__enter__()
     Lk = B[:, :k]
     G = torch.zeros((k, k), dtype=torch.float64, device=dev)
     for cs in range(0, k, chunk):
@@ -617,6 +624,7 @@ def chfsi_lean(A, k, tol=1e-6, Q=None, precision="mixed", degree=None, guard=Non
         ce = min(cs + chunk, k)
         R = A.matmul(B[:, cs:ce].contiguous(), prec=64) - B[:, cs:ce] * thd[cs:ce][None, :]
         worst = max(worst, float(torch.linalg.vector_norm(R, dim=0).max()) / b_up)
+    ph_final.__exit__(None, None, None)
     evals = torch.from_numpy(thf.copy()).to(dev)
     V = B[:, :k]
     if return_info:
