@@ -534,7 +534,12 @@ def chfsi_lean(A, k, tol=1e-6, Q=None, precision="mixed", degree=None, guard=Non
         for cs in range(L, p, chunk):
             ce = min(cs + chunk, p)
             with ph("rr_spmm"):
-                HYc = A.matmul(B[:, cs:ce].contiguous(), prec=64)
+                if prec == 32:
+                    # in-loop Rayleigh-Ritz on the FP32 store, as chfsi() does: the FP64
+                    # residuals below decide locking and the final pass is FP64 throughout
+                    HYc = A.matmul(B[:, cs:ce].to(torch.float32).contiguous(), prec=32).to(torch.float64)
+                else:
+                    HYc = A.matmul(B[:, cs:ce].contiguous(), prec=64)
             with ph("rr_gram"):
                 G[:, cs - L:ce - L] = B[:, L:].t() @ HYc
             del HYc

@@ -194,3 +194,68 @@ def band_slices(rowptr, cols, n_atoms, maxleafsize=100, gap=100):
         out[b] = [(bounds[t], bounds[t + 1]) for t in range(0, len(bounds), 2)]
     halfnnz = (((total - n_atoms) / 2) + n_atoms) * 9
     return out, halfnnz
+
+
+# ---------------------------------------------------------------------------
+# C restatement of neighbor_lists / cuthill_mckee (oracle/graph_c.c) for inputs
+# of millions of atoms; compiled with gcc on first use into oracle/_build/.
+# ---------------------------------------------------------------------------
+_CLIB = None
+
+
+def _clib():
+    global _CLIB
+    if _CLIB is not None:
+        return _CLIB
+    import ctypes
+    import os
+    import subprocess
+    here = os.path.dirname(os.path.abspath(__file__))
+    src = os.path.join(here, "graph_c.c")
+    out_dir = os.path.join(here, "_build")
+    so = os.path.join(out_dir, "liboracle_graph.so")
+    if not os.path.exists(so) or os.path.getmtime(so) < os.path.getmtime(src):
+        os.makedirs(out_dir, exist_ok=True)
+        tmp = so + f".{os.getpid()}.tmp"
+        subprocess.run(["gcc", "-O2", "-shared", "-fPIC", "-o", tmp, src, "-lm"], check=True)
+        os.replace(tmp, so)
+    L = ctypes.CDLL(so)
+    P = ctypes.c_void_p
+    L.oracle_neighbor_count.restype = ctypes.c_int64
+    L.oracle_neighbor_count.argtypes = [P, ctypes.c_int64, ctypes.c_double, P, P]
+    L.oracle_neighbor_fill.restype = ctypes.c_int
+    L.oracle_neighbor_fill.argtypes = [P, ctypes.c_int64, ctypes.c_double, P, P]
+    L.oracle_cuthill_mckee.restype = ctypes.c_int
+    L.oracle_cuthill_mckee.argtypes = [ctypes.c_int64, P, P, P, P, P]
+    _CLIB = L
+    return L
+
+
+def neighbor_lists_c(X_nm: np.ndarray, rc_gamma_A: float = 8.0):
+    """neighbor_lists() in C: (degree int32, rowptr int64, cols int32)."""
+    L = _clib()
+    X = np.ascontiguousarray(X_nm, dtype=np.float64)
+    n = X.shape[0]
+    rc = rc_gamma_A / 10.0
+    deg = np.zeros(n, np.int32)
+    rowptr = np.zeros(n + 1, np.int64)
+    nnz = L.oracle_neighbor_count(X.ctypes.data, n, rc, deg.ctypes.data, rowptr.ctypes.data)
+    assert nnz >= 0, "oracle_neighbor_count failed"
+    cols = np.zeros(max(nnz, 1), np.int32)[:nnz]
+    assert L.oracle_neighbor_fill(X.ctypes.data, n, rc, rowptr.ctypes.data, cols.ctypes.data) == 0
+    return deg, rowptr, cols
+
+
+def cuthill_mckee_c(rowptr, cols, degree, seed_order=None):
+    """cuthill_mckee(..., reverse=True) in C: (order int64, undo int64)."""
+    L = _clib()
+    rowptr = np.ascontiguousarray(rowptr, dtype=np.int64)
+    cols = np.ascontiguousarray(cols, dtype=np.int32)
+    degree = np.ascontiguousarray(degree, dtype=np.int32)
+    n = degree.shape[0]
+    seeds = np.ascontiguousarray(np.argsort(degree) if seed_order is None else seed_order, dtype=np.int64)
+    order = np.zeros(n, np.int64)
+    rc = L.oracle_cuthill_mckee(n, rowptr.ctypes.data, cols.ctypes.data, degree.ctypes.data, seeds.ctypes.data,
+                                order.ctypes.data)
+    assert rc == 0, f"oracle_cuthill_mckee failed ({rc})"
+    return order, np.argsort(order)

@@ -110,3 +110,27 @@ def test_limits_and_bad_input_raise():
     bad = torch.zeros(deg.shape[0], dtype=torch.int64, device="cuda")
     with pytest.raises(AssertionError, match="permutation"):
         _native().cuthill_mckee(rowptr, cols, deg, bad)
+
+
+def test_graph_full_size_cube2400k():
+    """The largest configuration (2,400,000 atoms, 300 touching globules in a cube;
+    81 Cuthill-McKee levels and a band of ~62k atoms, unlike the 100k assembly):
+    degrees equal scipy cKDTree's (the reference's neighbour engine), the lists
+    equal the C restatement of the oracle, and the Cuthill-McKee order and its
+    inverse equal the oracle's, bit for bit."""
+    from scipy.spatial import cKDTree
+    from inching_b200 import graph, synth
+    X = synth.workload("cube2400k") / 10.0
+    deg, rowptr, cols = graph.neighbor_lists(X, 8.0)
+    deg_h = deg.cpu().numpy()
+    ref_len = cKDTree(X).query_ball_point(X, 0.8, p=2.0, eps=0, return_length=True, workers=-1)
+    assert np.array_equal(deg_h, ref_len.astype(np.int32))
+    d_c, rp_c, c_c = og.neighbor_lists_c(X, 8.0)
+    assert np.array_equal(deg_h, d_c)
+    assert np.array_equal(rowptr.cpu().numpy(), rp_c)
+    assert np.array_equal(cols.cpu().numpy(), c_c)
+    seeds = np.argsort(d_c)
+    order, undo, levels = _native().cuthill_mckee(rowptr, cols, deg, torch.from_numpy(seeds).cuda())
+    o_ref, u_ref = og.cuthill_mckee_c(rp_c, c_c, d_c, seed_order=seeds)
+    assert np.array_equal(order.cpu().numpy(), o_ref)
+    assert np.array_equal(undo.cpu().numpy(), u_ref)
