@@ -192,17 +192,93 @@ __device__ __forceinline__ void vld(const T* p, T (&x)[V]) {
   }
 }
 
+// Rows handed out per grab of the row counter (in multiples of a block's rows
+// per step): all SMs then work on one compact frontier of consecutive rows, so
+// the X_j rows they gather stay an L2-sized window however far the blocks would
+// drift apart under a fixed grid stride.
+constexpr int kRowSteps = 4;
+
+template <class T, int B, int V, int NT>
+__device__ __forceinline__ void cols_row(int64_t i, const int64_t* __restrict__ rowptr, const void* __restrict__ ent,
+                                         const T* __restrict__ diag, const T* __restrict__ X, int64_t ldx, T* Y,
+                                         int64_t ldy, const T* Yin, int64_t ldyin, T* __restrict__ Acc,
+                                         int64_t ldacc, int c0, const Epi& ep, const double* __restrict__ Q,
+                                         int64_t ndof, const double* s_coef, int cl) {
+  constexpr int LPR = (B / V) < 32 ? (B / V) : 32;
+  constexpr int CPL = B / (LPR * V);
+    T acc[3][CPL][V];
+#pragma unroll
+  for (int t = 0; t < CPL; ++t)
+#pragma unroll
+    for (int v = 0; v < V; ++v) acc[0][t][v] = acc[1][t][v] = acc[2][t][v] = T(0);
+  const int64_t e1 = rowptr[i + 1];
+  const T* Xc = X + c0 + cl * V;
+#pragma unroll 2
+  for (int64_t e = rowptr[i]; e < e1; ++e) {
+    T wx, wy, wz;
+    int j;
+    Ent<T>::load(ent, e, wx, wy, wz, j);
+    const T* xj = Xc + 3 * (int64_t)j * ldx;
+#pragma unroll
+    for (int t = 0; t < CPL; ++t) {
+      T x0[V], x1[V], x2[V];
+      vld<T, V>(xj + t * LPR * V, x0);
+      vld<T, V>(xj + ldx + t * LPR * V, x1);
+      vld<T, V>(xj + 2 * ldx + t * LPR * V, x2);
+#pragma unroll
+      for (int v = 0; v < V; ++v) {
+        const T dot = wx * x0[v] + wy * x1[v] + wz * x2[v];
+        acc[0][t][v] -= wx * dot;
+        acc[1][t][v] -= wy * dot;
+        acc[2][t][v] -= wz * dot;
+      }
+    }
+  }
+  const T* d = diag + 8 * i;
+  const T dxx = d[0], dyy = d[1], dzz = d[2], dxy = d[3], dxz = d[4], dyz = d[5];
+  const int64_t r0 = 3 * i;
+#pragma unroll
+  for (int t = 0; t < CPL; ++t) {
+#pragma unroll
+    for (int v = 0; v < V; ++v) {
+      const int c = (t * LPR + cl) * V + v;
+      const T x0 = X[r0 * ldx + c0 + c], x1 = X[(r0 + 1) * ldx + c0 + c], x2 = X[(r0 + 2) * ldx + c0 + c];
+      T h[3];
+      h[0] = acc[0][t][v] + dxx * x0 + dxy * x1 + dxz * x2;
+      h[1] = acc[1][t][v] + dxy * x0 + dyy * x1 + dyz * x2;
+      h[2] = acc[2][t][v] + dxz * x0 + dyz * x1 + dzz * x2;
+      const T xs[3] = {x0, x1, x2};
+#pragma unroll
+      for (int a = 0; a < 3; ++a) {
+        const int64_t row = r0 + a;
+        double al = ep.alpha, ga = ep.gamma, be = ep.beta;
+      if (ep.seg_coef != nullptr) {
+        const int sg = __ldg(ep.atom_seg + i);
+        al = __ldg(ep.seg_coef + 3 * sg);
+        ga = __ldg(ep.seg_coef + 3 * sg + 1);
+        be = __ldg(ep.seg_coef + 3 * sg + 2);
+      }
+      double y = al * (double)h[a] + ga * (double)xs[a];
+        if (ep.has_yin) y += be * (double)Yin[row * ldyin + c0 + c];
+        for (int q = 0; q < ep.r; ++q) y += Q[q * ndof + row] * s_coef[q * B + c];
+        Y[row * ldy + c0 + c] = (T)y;
+        if (ep.accumulate) Acc[row * ldacc + c0 + c] += (T)(ep.mu * y);
+      }
+    }
+  }
+}
+
 template <class T, int B, int V, int NT>
 __global__ void __launch_bounds__(NT)
 k_spmm_cols(int64_t n_atoms, const int64_t* __restrict__ rowptr, const void* __restrict__ ent,
             const T* __restrict__ diag, const T* __restrict__ X, int64_t ldx, T* Y, int64_t ldy, const T* Yin,
             int64_t ldyin, T* __restrict__ Acc, int64_t ldacc, int c0, Epi ep, const double* __restrict__ Q,
-            int64_t ndof, const double* __restrict__ coef) {
+            int64_t ndof, const double* __restrict__ coef, int* __restrict__ row_counter) {
   constexpr int LPR = (B / V) < 32 ? (B / V) : 32;
-  constexpr int CPL = B / (LPR * V);
   constexpr int RPW = 32 / LPR;
   constexpr int GPB = (NT / 32) * RPW;
   __shared__ double s_coef[8 * B];
+  __shared__ int s_row;
   if (ep.r > 0) {
     for (int t = threadIdx.x; t < ep.r * B; t += NT) s_coef[t] = coef[t];
     __syncthreads();
@@ -210,69 +286,26 @@ k_spmm_cols(int64_t n_atoms, const int64_t* __restrict__ rowptr, const void* __r
   const int lane = threadIdx.x & 31;
   const int cl = lane % LPR;
   const int grp = (threadIdx.x >> 5) * RPW + lane / LPR;
-  // Block-interleaved rows: at any time the whole grid works on one band of
-  // consecutive rows, so the X_j rows it gathers stay an L2-sized window even
-  // when X itself is many times larger than L2.
-  for (int64_t i = (int64_t)blockIdx.x * GPB + grp; i < n_atoms; i += (int64_t)gridDim.x * GPB) {
-    T acc[3][CPL][V];
-#pragma unroll
-    for (int t = 0; t < CPL; ++t)
-#pragma unroll
-      for (int v = 0; v < V; ++v) acc[0][t][v] = acc[1][t][v] = acc[2][t][v] = T(0);
-    const int64_t e1 = rowptr[i + 1];
-    const T* Xc = X + c0 + cl * V;
-#pragma unroll 2
-    for (int64_t e = rowptr[i]; e < e1; ++e) {
-      T wx, wy, wz;
-      int j;
-      Ent<T>::load(ent, e, wx, wy, wz, j);
-      const T* xj = Xc + 3 * (int64_t)j * ldx;
-#pragma unroll
-      for (int t = 0; t < CPL; ++t) {
-        T x0[V], x1[V], x2[V];
-        vld<T, V>(xj + t * LPR * V, x0);
-        vld<T, V>(xj + ldx + t * LPR * V, x1);
-        vld<T, V>(xj + 2 * ldx + t * LPR * V, x2);
-#pragma unroll
-        for (int v = 0; v < V; ++v) {
-          const T dot = wx * x0[v] + wy * x1[v] + wz * x2[v];
-          acc[0][t][v] -= wx * dot;
-          acc[1][t][v] -= wy * dot;
-          acc[2][t][v] -= wz * dot;
-        }
-      }
-    }
-    const T* d = diag + 8 * i;
-    const T dxx = d[0], dyy = d[1], dzz = d[2], dxy = d[3], dxz = d[4], dyz = d[5];
-    const int64_t r0 = 3 * i;
-#pragma unroll
-    for (int t = 0; t < CPL; ++t) {
-#pragma unroll
-      for (int v = 0; v < V; ++v) {
-        const int c = (t * LPR + cl) * V + v;
-        const T x0 = X[r0 * ldx + c0 + c], x1 = X[(r0 + 1) * ldx + c0 + c], x2 = X[(r0 + 2) * ldx + c0 + c];
-        T h[3];
-        h[0] = acc[0][t][v] + dxx * x0 + dxy * x1 + dxz * x2;
-        h[1] = acc[1][t][v] + dxy * x0 + dyy * x1 + dyz * x2;
-        h[2] = acc[2][t][v] + dxz * x0 + dyz * x1 + dzz * x2;
-        const T xs[3] = {x0, x1, x2};
-#pragma unroll
-        for (int a = 0; a < 3; ++a) {
-          const int64_t row = r0 + a;
-          double al = ep.alpha, ga = ep.gamma, be = ep.beta;
-        if (ep.seg_coef != nullptr) {
-          const int sg = __ldg(ep.atom_seg + i);
-          al = __ldg(ep.seg_coef + 3 * sg);
-          ga = __ldg(ep.seg_coef + 3 * sg + 1);
-          be = __ldg(ep.seg_coef + 3 * sg + 2);
-        }
-        double y = al * (double)h[a] + ga * (double)xs[a];
-          if (ep.has_yin) y += be * (double)Yin[row * ldyin + c0 + c];
-          for (int q = 0; q < ep.r; ++q) y += Q[q * ndof + row] * s_coef[q * B + c];
-          Y[row * ldy + c0 + c] = (T)y;
-          if (ep.accumulate) Acc[row * ldacc + c0 + c] += (T)(ep.mu * y);
-        }
-      }
+  if (row_counter == nullptr) {
+    // fixed block-interleaved stride: at any time the grid works on one band of
+    // consecutive rows (used where no workspace holds a counter)
+    for (int64_t i = (int64_t)blockIdx.x * GPB + grp; i < n_atoms; i += (int64_t)gridDim.x * GPB)
+      cols_row<T, B, V, NT>(i, rowptr, ent, diag, X, ldx, Y, ldy, Yin, ldyin, Acc, ldacc, c0, ep, Q, ndof, s_coef,
+                            cl);
+    return;
+  }
+  for (;;) {
+    if (threadIdx.x == 0) s_row = atomicAdd(row_counter, GPB * kRowSteps);
+    __syncthreads();
+    const int64_t base = s_row;
+    __syncthreads();                     // every thread has read s_row before the next grab
+    if (base >= n_atoms) break;
+#pragma unroll 1
+    for (int st = 0; st < kRowSteps; ++st) {
+      const int64_t i = base + st * GPB + grp;
+      if (i < n_atoms)
+        cols_row<T, B, V, NT>(i, rowptr, ent, diag, X, ldx, Y, ldy, Yin, ldyin, Acc, ldacc, c0, ep, Q, ndof,
+                              s_coef, cl);
     }
   }
 }
@@ -426,7 +459,7 @@ template <class T, int B, int G>
 cudaError_t launch_tile(int64_t n_atoms, const int64_t* rowptr, const void* ent, const T* diag, const T* X,
                         int64_t ldx, T* Y, int64_t ldy, const T* Yin, int64_t ldyin, T* Acc, int64_t ldacc, int c0,
                         Epi ep, const double* Q, double hot_shift, double* partial, double* coef,
-                        cudaStream_t stream) {
+                        cudaStream_t stream, int* row_counter) {
   const int64_t ndof = 3 * n_atoms;
   if (ep.r > 0) {
     dim3 g(kQxBlocks, ep.r);
@@ -444,15 +477,21 @@ cudaError_t launch_tile(int64_t n_atoms, const int64_t* rowptr, const void* ent,
     if (ep.accumulate) vec = vec && (ldacc % 2 == 0) && ((uintptr_t)Acc % al == 0);
     const int nt = g_cols_threads.load();
     const int bps = g_cols_blocks_per_sm.load();
+    if (row_counter != nullptr) {
+      const cudaError_t me = cudaMemsetAsync(row_counter, 0, sizeof(int), stream);
+      if (me != cudaSuccess) return me;
+    }
 #define COLS_LAUNCH(NTV)                                                                                     \
   {                                                                                                           \
     const int blocks = grid_for(n_atoms, 4 * NTV / 32, 148 * bps);                                            \
     if (vec)                                                                                                  \
       k_spmm_cols<T, B, 2, NTV><<<blocks, NTV, 0, stream>>>(n_atoms, rowptr, ent, diag, X, ldx, Y, ldy, Yin,   \
-                                                            ldyin, Acc, ldacc, c0, ep, Q, ndof, coef);       \
+                                                            ldyin, Acc, ldacc, c0, ep, Q, ndof, coef,        \
+                                                            row_counter);                                    \
     else                                                                                                      \
       k_spmm_cols<T, B, 1, NTV><<<blocks, NTV, 0, stream>>>(n_atoms, rowptr, ent, diag, X, ldx, Y, ldy, Yin,   \
-                                                            ldyin, Acc, ldacc, c0, ep, Q, ndof, coef);       \
+                                                            ldyin, Acc, ldacc, c0, ep, Q, ndof, coef,        \
+                                                            row_counter);                                    \
   }
     const int wmode = g_warp_kernel.load();
     if (wmode > 0 && B >= 32 && (vec || B >= 32)) {
@@ -484,7 +523,8 @@ cudaError_t launch_tile(int64_t n_atoms, const int64_t* rowptr, const void* ent,
 template <class T>
 cudaError_t run(int64_t n_atoms, const int64_t* rowptr, const void* ent, const void* diag, const void* Xv,
                 int64_t ldx, int b, void* Yv, int64_t ldy, const void* Yinv, int64_t ldyin, void* Accv, int64_t ldacc,
-                Epi ep, const double* Q, double hot_shift, double* partial, double* coef, cudaStream_t s) {
+                Epi ep, const double* Q, double hot_shift, double* partial, double* coef, cudaStream_t s,
+                int* row_counter = nullptr) {
   const T* X = static_cast<const T*>(Xv);
   T* Y = static_cast<T*>(Yv);
   const T* Yin = static_cast<const T*>(Yinv);
@@ -496,7 +536,7 @@ cudaError_t run(int64_t n_atoms, const int64_t* rowptr, const void* ent, const v
     const int rem = b - c0;
 #define TILE(BB, GG)                                                                                          \
   e = launch_tile<T, BB, GG>(n_atoms, rowptr, ent, D, X, ldx, Y, ldy, Yin, ldyin, Acc, ldacc, c0, ep, Q,     \
-                             hot_shift, partial, coef, s);                                                     \
+                             hot_shift, partial, coef, s, row_counter);                                        \
   c0 += BB;
     bool done64 = false;
     if constexpr (sizeof(T) == 4) {
@@ -540,6 +580,7 @@ extern "C" size_t inch_spmm_workspace_size(int64_t n_atoms, int32_t b, int32_t r
   (void)n_atoms;
   (void)b;
   Sizer s;
+  s.take<int>(1);                              // row counter of the wide-block kernel
   s.take<double>((size_t)kQxBlocks * 8 * 64);  // partial sums (r <= 8, tile <= 64)
   s.take<double>(8 * 64);                      // coefficients
   (void)r;
@@ -563,9 +604,14 @@ extern "C" inch_status inch_spmm(int32_t prec, int64_t n_atoms, const int64_t* r
   INCH_REQUIRE(!e.accumulate || (Acc != nullptr && ldacc >= b), INCH_INVALID_ARG, "inch_spmm: accumulate needs Acc");
   INCH_REQUIRE(((uintptr_t)ent & 15) == 0 && ((uintptr_t)diag & 15) == 0, INCH_INVALID_ARG,
                "inch_spmm: store buffers must be 16-byte aligned");
+  // The workspace (when given) holds the wide kernel's row counter and the
+  // Hotelling scratch; without one (allowed for r = 0) the wide kernel walks its
+  // rows with a fixed grid stride instead of the counter.
   double *partial = nullptr, *coef = nullptr;
-  if (e.r > 0) {
+  int* counter = nullptr;
+  if (ws != nullptr || e.r > 0) {
     Carver c(ws, ws_bytes);
+    counter = c.take<int>(1);
     partial = c.take<double>((size_t)kQxBlocks * 8 * 64);
     coef = c.take<double>(8 * 64);
     INCH_REQUIRE(c.ok, INCH_OOM, "inch_spmm: workspace of %zu bytes, need %zu", ws_bytes,
@@ -575,10 +621,10 @@ extern "C" inch_status inch_spmm(int32_t prec, int64_t n_atoms, const int64_t* r
   cudaError_t err;
   if (prec == 32)
     err = run<float>(n_atoms, rowptr, ent, diag, X, ldx, b, Y, ldy, Yin, ldyin, Acc, ldacc, ep, q, e.hot_shift,
-                     partial, coef, stream);
+                     partial, coef, stream, counter);
   else
     err = run<double>(n_atoms, rowptr, ent, diag, X, ldx, b, Y, ldy, Yin, ldyin, Acc, ldacc, ep, q, e.hot_shift,
-                      partial, coef, stream);
+                      partial, coef, stream, counter);
   INCH_REQUIRE(err == cudaSuccess, INCH_CUDA_ERROR, "inch_spmm: %s", cudaGetErrorString(err));
   return INCH_OK;
 }
