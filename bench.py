@@ -62,6 +62,8 @@ def parse():
                     "solver's size rule)")
     ap.add_argument("--profile", action="store_true", help="cube2400k: CUDA-event phase times of the solver")
     ap.add_argument("--layout", default="tiles", choices=["tiles", "pairs"], help="store layout for --kernel-only")
+    ap.add_argument("--traversal", type=int, default=None, choices=[0, 1, 2],
+                    help="row traversal of the wide pair kernel (--kernel-only)")
     ap.add_argument("--band-panel", type=int, default=None, choices=[64, 128],
                     help="widest FP32 panel of the band-tile product (--kernel-only)")
     return ap.parse_args()
@@ -75,9 +77,9 @@ def run_kernel_only(args):
     from inching_b200 import graph, synth
     from inching_b200.hessian import HessianStore
     from inching_b200 import _native
-    if args.tune:
-        t, bps = (int(x) for x in args.tune.split(","))
-        _native.spmm_tune(t, bps)
+    if args.tune or args.traversal is not None:
+        t, bps = (int(x) for x in (args.tune or "256,5").split(","))
+        _native.spmm_tune(t, bps, args.traversal)
     if args.band_panel:
         _native.spmm_band_tune(args.band_panel)
     Xd = torch.from_numpy(synth.workload(args.workload) / 10.0).cuda()
@@ -100,6 +102,7 @@ def run_kernel_only(args):
     nbytes = H.store_bytes(prec, args.b) + 2 * X.numel() * X.element_size()
     best = min(ms)
     print(json.dumps({"kernel": args.kernel_only, "b": args.b, "tune": args.tune, "layout": args.layout,
+                      "traversal": args.traversal,
                       "band_panel": args.band_panel, "n_atoms": H.n_atoms,
                       "nnz": H.nnz_blocks,
                       "ms": [round(m, 4) for m in ms], "algorithmic_bytes": nbytes,

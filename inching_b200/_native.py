@@ -94,6 +94,7 @@ _SIGS = {
                                              c_void_p, c_void_p, c_void_p, c_void_p, c_void_p]),
     "inch_spmm_workspace_size": (c_size_t, [c_int64, c_int32, c_int32]),
     "inch_spmm_tune": (ctypes.c_int, [c_int32, c_int32]),
+    "inch_spmm_traversal": (ctypes.c_int, [c_int32]),
     "inch_spmm_seg": (ctypes.c_int, [c_int32, c_int64, c_void_p, c_void_p, c_void_p, c_void_p, c_int64, c_int32,
                                      c_void_p, c_int64, c_void_p, c_int64, c_void_p, c_void_p, c_void_p]),
     "inch_spmm": (ctypes.c_int, [c_int32, c_int64, c_void_p, c_void_p, c_void_p, c_void_p, c_int64, c_int32,
@@ -326,9 +327,20 @@ def spmm_seg(prec, n_atoms, rowptr, ent, diag, X, Y, atom_seg, seg_coef, Yin=Non
     return Y
 
 
-def spmm_tune(threads_per_block=256, blocks_per_sm=5):
-    """Set the wide-block SpMM launch shape for this process (autotuner hook)."""
+_spmm_setting = [None]
+
+
+def spmm_tune(threads_per_block=256, blocks_per_sm=5, traversal=None):
+    """Set the wide-block SpMM launch shape (and, if given, the row traversal: 0
+    fixed stride, 1 per-warp chunks, 2 per-block chunks) for this process
+    (autotuner hook)."""
+    setting = (threads_per_block, blocks_per_sm, traversal)
+    if _spmm_setting[0] == setting:
+        return
     check(lib().inch_spmm_tune(threads_per_block, blocks_per_sm))
+    if traversal is not None:
+        check(lib().inch_spmm_traversal(traversal))
+    _spmm_setting[0] = setting
 
 
 def spmm(prec, n_atoms, rowptr, ent, diag, X, Y, *, alpha=1.0, gamma=0.0, beta=0.0, Yin=None,

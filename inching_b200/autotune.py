@@ -2,12 +2,18 @@
 
 For a given store, block width and precision it times the candidate launch
 configurations of the SpMM with CUDA events on the current stream and keeps the
-fastest for the process:
-  * layout: the pair layout (one entry per neighbour pair) or the row-tile layout
+fastest, for the process and on the store itself (the store re-applies its own
+choice before each product, so stores of different sizes keep their own):
+  * layout: the pair layout (one entry per neighbour pair) or the band-tile layout
     (8-row tiles with merged neighbour unions), when the store has tiles;
-  * lane-group kernel block shape: 256 x 5, 256 x 4, 512 x 2, 1024 x 1 blocks/SM;
-  * the whole-warp-row kernel with batched gathers ("warp", for >= 32 columns).
+  * lane-group kernel block shape: 256 x 5, 256 x 4, 512 x 2 blocks/SM;
+  * row traversal of the lane-group kernel: fixed grid stride (the warps of a
+    block on neighbouring rows share their X_j rows in L1), or chunks of rows
+    from a counter per warp or per block (one compact frontier over all SMs keeps
+    the X_j rows in L2 on large structures);
+  * the whole-warp-row kernel with batched gathers ("pairs", 0, ...).
 Results are cached per (atoms, pairs, width class, precision, device name).
+The solvers call tune_spmm once per store for the widths they use.
 """
 from __future__ import annotations
 
@@ -15,8 +21,9 @@ import torch
 
 from . import _native
 
-CANDIDATES = (("pairs", 256, 5), ("pairs", 256, 4), ("pairs", 512, 2), ("pairs", 1024, 1), ("pairs", 0, 4),
-              ("tiles", 256, 5))
+# (layout, threads per block (0: whole-warp kernel), blocks per SM, traversal)
+CANDIDATES = (("pairs", 256, 5, 1), ("pairs", 256, 5, 0), ("pairs", 256, 5, 2), ("pairs", 256, 4, 1),
+              ("pairs", 512, 2, 1), ("pairs", 0, 4, 0), ("tiles", 256, 5, 1))
 _cache = {}
 
 
@@ -25,8 +32,14 @@ def _width_class(b):
 
 
 def _apply(H, cfg):
-    layout, threads, bps = cfg
-    _native.spmm_tune(threads, bps)
+    apply_config(H, cfg)
+
+
+def apply_config(H, cfg):
+    """Make cfg = (layout, threads, blocks per SM, traversal) the current choice."""
+    layout, threads, bps, trav = cfg
+    if layout == "pairs":
+        _native.spmm_tune(threads, bps, trav)
     H.use_tiles = layout == "tiles"
 
 
@@ -54,6 +67,7 @@ def tune_spmm(H, b, prec=32, reps=3, candidates=CANDIDATES, timer=cuda_event_ms)
     key = (H.n_atoms, H.nnz_blocks, _width_class(b), prec, _device_name(H.device))
     if key in _cache:
         _apply(H, _cache[key][0])
+        _remember(H, prec, b, _cache[key][0])
         return _cache[key]
     dt = torch.float64 if prec == 64 else torch.float32
     w = _width_class(b) if b >= 8 else b
@@ -63,16 +77,25 @@ def tune_spmm(H, b, prec=32, reps=3, candidates=CANDIDATES, timer=cuda_event_ms)
     for cfg in candidates:
         if cfg[0] == "tiles" and H.tiles is None:
             continue
+        if cfg[0] == "pairs" and not H.keep_pairs:
+            continue
         _apply(H, cfg)
         table[cfg] = timer(lambda: H.matmul(X, out=Y, prec=prec), reps)
     best = min(table, key=table.get)
     _apply(H, best)
+    _remember(H, prec, b, best)
     _cache[key] = (best, table)
     return best, table
 
 
+def _remember(H, prec, b, cfg):
+    cfgs = getattr(H, "spmm_cfg", None)
+    if cfgs is not None:
+        cfgs[(prec, _width_class(b))] = cfg
+
+
 def reset():
     """Forget the cached choices and restore the default launch shape (256 x 5,
-    pair layout kernel)."""
+    pair layout kernel, per-warp row chunks)."""
     _cache.clear()
-    _native.spmm_tune(256, 5)
+    _native.spmm_tune(256, 5, 1)

@@ -81,6 +81,10 @@ constexpr int kThreads = 256;
 std::atomic<int> g_cols_threads{256};
 std::atomic<int> g_cols_blocks_per_sm{5};
 std::atomic<int> g_warp_kernel{0};   // 1: whole-warp rows with batched gathers where B/V >= 32
+// Row traversal of the wide-block kernel when a workspace holds a row counter:
+// 0 fixed block-interleaved stride, 1 per-warp chunks from the counter, 2 per-block
+// chunks from the counter (set by inch_spmm_traversal, the autotuner's hook).
+std::atomic<int> g_cols_traversal{1};
 
 template <class T, int B, int G>
 __global__ void __launch_bounds__(kThreads)
@@ -192,10 +196,11 @@ __device__ __forceinline__ void vld(const T* p, T (&x)[V]) {
   }
 }
 
-// Rows handed out per grab of the row counter (in multiples of a block's rows
-// per step): all SMs then work on one compact frontier of consecutive rows, so
-// the X_j rows they gather stay an L2-sized window however far the blocks would
-// drift apart under a fixed grid stride.
+// Steps of rows a warp takes per grab of the row counter: warps take chunks of
+// consecutive rows in order, so all SMs work on one compact frontier and the
+// X_j rows they gather stay an L2-sized window, however far blocks would drift
+// apart under a fixed grid stride (on the 2.4M-atom cube the fixed stride read
+// 11x the algorithmic bytes from DRAM).
 constexpr int kRowSteps = 4;
 
 template <class T, int B, int V, int NT>
@@ -273,7 +278,7 @@ __global__ void __launch_bounds__(NT)
 k_spmm_cols(int64_t n_atoms, const int64_t* __restrict__ rowptr, const void* __restrict__ ent,
             const T* __restrict__ diag, const T* __restrict__ X, int64_t ldx, T* Y, int64_t ldy, const T* Yin,
             int64_t ldyin, T* __restrict__ Acc, int64_t ldacc, int c0, Epi ep, const double* __restrict__ Q,
-            int64_t ndof, const double* __restrict__ coef, int* __restrict__ row_counter) {
+            int64_t ndof, const double* __restrict__ coef, int* __restrict__ row_counter, int traversal) {
   constexpr int LPR = (B / V) < 32 ? (B / V) : 32;
   constexpr int RPW = 32 / LPR;
   constexpr int GPB = (NT / 32) * RPW;
@@ -286,23 +291,44 @@ k_spmm_cols(int64_t n_atoms, const int64_t* __restrict__ rowptr, const void* __r
   const int lane = threadIdx.x & 31;
   const int cl = lane % LPR;
   const int grp = (threadIdx.x >> 5) * RPW + lane / LPR;
-  if (row_counter == nullptr) {
-    // fixed block-interleaved stride: at any time the grid works on one band of
-    // consecutive rows (used where no workspace holds a counter)
+  if (row_counter == nullptr || traversal == 0) {
+    // fixed block-interleaved stride: the grid starts on one band of consecutive
+    // rows, each block's warps on neighbouring rows (their X_j rows shared in L1)
     for (int64_t i = (int64_t)blockIdx.x * GPB + grp; i < n_atoms; i += (int64_t)gridDim.x * GPB)
       cols_row<T, B, V, NT>(i, rowptr, ent, diag, X, ldx, Y, ldy, Yin, ldyin, Acc, ldacc, c0, ep, Q, ndof, s_coef,
                             cl);
     return;
   }
+  if (traversal == 2) {
+    // each block takes a chunk of kRowSteps * GPB consecutive rows, its warps on
+    // neighbouring rows (compact frontier and L1 sharing, one barrier per chunk)
+    for (;;) {
+      if (threadIdx.x == 0) s_row = atomicAdd(row_counter, GPB * kRowSteps);
+      __syncthreads();
+      const int64_t base = s_row;
+      __syncthreads();                   // every thread has read s_row before the next grab
+      if (base >= n_atoms) break;
+#pragma unroll 1
+      for (int st = 0; st < kRowSteps; ++st) {
+        const int64_t i = base + st * GPB + grp;
+        if (i < n_atoms)
+          cols_row<T, B, V, NT>(i, rowptr, ent, diag, X, ldx, Y, ldy, Yin, ldyin, Acc, ldacc, c0, ep, Q, ndof,
+                                s_coef, cl);
+      }
+    }
+    return;
+  }
+  // each warp takes its own chunk of kRowSteps * RPW consecutive rows (no block
+  // barrier, so a long row holds back only its own warp)
+  const int wg = lane / LPR;
   for (;;) {
-    if (threadIdx.x == 0) s_row = atomicAdd(row_counter, GPB * kRowSteps);
-    __syncthreads();
-    const int64_t base = s_row;
-    __syncthreads();                     // every thread has read s_row before the next grab
+    int base = 0;
+    if (lane == 0) base = atomicAdd(row_counter, RPW * kRowSteps);
+    base = __shfl_sync(0xffffffffu, base, 0);
     if (base >= n_atoms) break;
 #pragma unroll 1
     for (int st = 0; st < kRowSteps; ++st) {
-      const int64_t i = base + st * GPB + grp;
+      const int64_t i = (int64_t)base + st * RPW + wg;
       if (i < n_atoms)
         cols_row<T, B, V, NT>(i, rowptr, ent, diag, X, ldx, Y, ldy, Yin, ldyin, Acc, ldacc, c0, ep, Q, ndof,
                               s_coef, cl);
@@ -477,7 +503,8 @@ cudaError_t launch_tile(int64_t n_atoms, const int64_t* rowptr, const void* ent,
     if (ep.accumulate) vec = vec && (ldacc % 2 == 0) && ((uintptr_t)Acc % al == 0);
     const int nt = g_cols_threads.load();
     const int bps = g_cols_blocks_per_sm.load();
-    if (row_counter != nullptr) {
+    const int trav = row_counter != nullptr ? g_cols_traversal.load() : 0;
+    if (trav != 0) {
       const cudaError_t me = cudaMemsetAsync(row_counter, 0, sizeof(int), stream);
       if (me != cudaSuccess) return me;
     }
@@ -487,11 +514,11 @@ cudaError_t launch_tile(int64_t n_atoms, const int64_t* rowptr, const void* ent,
     if (vec)                                                                                                  \
       k_spmm_cols<T, B, 2, NTV><<<blocks, NTV, 0, stream>>>(n_atoms, rowptr, ent, diag, X, ldx, Y, ldy, Yin,   \
                                                             ldyin, Acc, ldacc, c0, ep, Q, ndof, coef,        \
-                                                            row_counter);                                    \
+                                                            row_counter, trav);                              \
     else                                                                                                      \
       k_spmm_cols<T, B, 1, NTV><<<blocks, NTV, 0, stream>>>(n_atoms, rowptr, ent, diag, X, ldx, Y, ldy, Yin,   \
                                                             ldyin, Acc, ldacc, c0, ep, Q, ndof, coef,        \
-                                                            row_counter);                                    \
+                                                            row_counter, trav);                              \
   }
     const int wmode = g_warp_kernel.load();
     if (wmode > 0 && B >= 32 && (vec || B >= 32)) {
@@ -573,6 +600,12 @@ extern "C" inch_status inch_spmm_tune(int32_t threads_per_block, int32_t blocks_
   INCH_REQUIRE(blocks_per_sm >= 1 && blocks_per_sm <= 8, INCH_INVALID_ARG, "inch_spmm_tune: blocks_per_sm in 1..8");
   g_cols_threads.store(threads_per_block);
   g_cols_blocks_per_sm.store(blocks_per_sm);
+  return INCH_OK;
+}
+
+extern "C" inch_status inch_spmm_traversal(int32_t mode) {
+  INCH_REQUIRE(mode >= 0 && mode <= 2, INCH_INVALID_ARG, "inch_spmm_traversal: mode must be 0, 1 or 2");
+  g_cols_traversal.store(mode);
   return INCH_OK;
 }
 

@@ -99,6 +99,8 @@ class HessianStore:
                 self.ent64 = None if self.ent64 is None else self.ent64[:0]
                 self.ent32 = None if self.ent32 is None else self.ent32[:0]
         self.keep_pairs = bool(keep_pairs)
+        # autotuned launch choice per (precision, width class), set by autotune.tune_spmm
+        self.spmm_cfg = {}
 
     # -- reference-compatible views ------------------------------------------------
     @property
@@ -157,6 +159,12 @@ class HessianStore:
             return out
         if out is None:
             out = torch.empty_like(X)
+        if self.spmm_cfg:
+            bw = 1 if X.dim() == 1 else X.shape[1]
+            cfg = self.spmm_cfg.get((prec, 64 if bw >= 64 else (32 if bw >= 32 else (8 if bw >= 8 else bw))))
+            if cfg is not None:
+                from .autotune import apply_config
+                apply_config(self, cfg)
         ent, diag = self.store(prec)
         probe = _probe if (_probe is not None and (_probe.prec is None or _probe.prec == prec)) else None
         if probe is not None:

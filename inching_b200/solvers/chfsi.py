@@ -42,6 +42,18 @@ from ..spectrum import estimate_spectrum_bound
 STALL_RESTART = 3    # iterations without a new lock before the locked + active Rayleigh-Ritz
 
 
+def autotune_store(A, precs):
+    """Time the wide-product launch choices once for this store (cached per store
+    size) at each precision the solver uses; no-op for operators that are not
+    Hessian stores on the GPU."""
+    if getattr(A, "spmm_cfg", None) is None or getattr(A, "device", None) is None or A.device.type != "cuda":
+        return
+    from ..autotune import tune_spmm
+    for prec in precs:
+        if A.has(prec):
+            tune_spmm(A, 64, prec=prec)
+
+
 def default_guard(k):
     """Guard vectors carried beyond the k wanted ones (a quarter of k, at least 16:
     the gap to the block's last Ritz value sets the filter's convergence rate)."""
@@ -324,6 +336,8 @@ def chfsi(A, k, tol=1e-6, Q=None, precision="mixed", degree=24, guard=None, maxi
     p = min(k + guard, n - (0 if Q is None else Q.shape[0]))
     Qd = None if Q is None else HessianOperator(A, Q=Q).Q
     ph = _Phases(profile)
+    with ph("autotune"):
+        autotune_store(A, sorted({prec, 64}))
     if spectrum_upper is None:
         with ph("bound"):
             lo, hi = estimate_spectrum_bound(A, steps=40, seed=seed + 1, precision=precision)
@@ -484,6 +498,7 @@ def chfsi_lean(A, k, tol=1e-6, Q=None, precision="mixed", degree=None, guard=Non
     if degree is None:
         degree = lean_degree(A, p)
     Qd = None if Q is None else HessianOperator(A, Q=Q).Q
+    autotune_store(A, sorted({prec, 64}))
     lo, hi = estimate_spectrum_bound(A, steps=40, seed=seed + 1, precision=precision)
     b_up = hi * 1.02 + 1e-3 * abs(hi)
     g = torch.Generator(device=dev)

@@ -235,6 +235,14 @@ typedef struct {
 } inch_spmm_epilogue;
 
 size_t inch_spmm_workspace_size(int64_t n_atoms, int32_t b, int32_t r);
+/* Row traversal of inch_spmm's wide-block kernel (b >= 8) for this process (the
+ * autotuner's hook; no reference counterpart): 0 a fixed block-interleaved grid
+ * stride; 1 (default) chunks of consecutive rows that each warp takes from a
+ * counter in the workspace; 2 chunks that each block takes from it.  Modes 1 and
+ * 2 keep every SM on one compact frontier of rows, so the gathered X rows stay
+ * in L2 on large structures; they need the workspace (calls without one use 0),
+ * and calls that share one workspace must not overlap on the GPU. */
+inch_status inch_spmm_traversal(int32_t mode);
 /* inch_spmm with per-segment coefficients (no reference counterpart): for a
  * block-diagonal store holding many structures, atom i uses (alpha, gamma, beta) =
  * seg_coef[3*atom_seg[i] .. +2] in Y = alpha*(H X) + gamma*X + beta*Yin, so each

@@ -1,12 +1,14 @@
-"""Autotuner host logic on CPU: the fastest candidate is applied, the choice is
-cached per (atoms, pairs, width class, precision, device), the row-tile layout
-is tried only when the store has tiles, and the launch-shape hook of the C ABI
-accepts the documented shapes and rejects others (no GPU call is involved)."""
+"""Autotuner host logic on CPU: the fastest candidate is applied and remembered
+on the store, the choice is cached per (atoms, pairs, width class, precision,
+device), the band-tile layout is tried only when the store has tiles, and the
+launch hooks of the C ABI accept the documented settings and reject others (no
+GPU call is involved)."""
 import pytest
 import torch
 
-COST = {("pairs", 256, 5): 3.0, ("pairs", 256, 4): 2.0, ("pairs", 512, 2): 2.5, ("pairs", 1024, 1): 4.0,
-        ("pairs", 0, 4): 1.5, ("tiles", 256, 5): 1.0}
+COST = {("pairs", 256, 5, 1): 3.0, ("pairs", 256, 5, 0): 2.2, ("pairs", 256, 5, 2): 2.9,
+        ("pairs", 256, 4, 1): 2.0, ("pairs", 512, 2, 1): 2.5, ("pairs", 0, 4, 0): 1.5,
+        ("tiles", 256, 5, 1): 1.0}
 
 
 class FakeStore:
@@ -16,6 +18,8 @@ class FakeStore:
         self.device = torch.device("cpu")
         self.tiles = {} if tiles else None
         self.use_tiles = False
+        self.keep_pairs = True
+        self.spmm_cfg = {}
         self.calls = 0
 
     def matmul(self, X, out=None, prec=32):
@@ -26,37 +30,46 @@ class FakeStore:
 
 def test_autotuner_picks_fastest_and_caches(monkeypatch):
     from inching_b200 import autotune
-    applied = []
-    monkeypatch.setattr(autotune._native, "spmm_tune", lambda t, b: applied.append((t, b)))
+    applied = [(256, 5, 1)]
+    monkeypatch.setattr(autotune._native, "spmm_tune", lambda t, b, tr=None: applied.append((t, b, tr)))
     autotune._cache.clear()
     timed = []
 
     def timer(fn, reps):
         fn()
-        cfg = (("tiles" if H.use_tiles else "pairs"),) + applied[-1]
+        cfg = ("tiles", 256, 5, 1) if H.use_tiles else (("pairs",) + applied[-1])
         timed.append(cfg)
         return COST[cfg]
 
     H = FakeStore(tiles=False)
     best, table = autotune.tune_spmm(H, 64, timer=timer)
-    assert best == ("pairs", 0, 4) and applied[-1] == (0, 4) and not H.use_tiles
-    assert set(table) == {c for c in COST if c[0] == "pairs"} and len(timed) == 5 and H.calls == 5
+    assert best == ("pairs", 0, 4, 0) and applied[-1] == (0, 4, 0) and not H.use_tiles
+    assert H.spmm_cfg[(32, 64)] == best
+    assert set(table) == {c for c in COST if c[0] == "pairs"} and len(timed) == 6 and H.calls == 6
     again = autotune.tune_spmm(H, 100, timer=timer)          # same width class (64): cached
-    assert again[0] == best and len(timed) == 5 and applied[-1] == (0, 4)
+    assert again[0] == best and len(timed) == 6 and applied[-1] == (0, 4, 0)
     autotune.tune_spmm(H, 16, timer=timer)                   # another width class: timed again
-    assert len(timed) == 10
+    assert len(timed) == 12 and (32, 8) in H.spmm_cfg
     H = FakeStore(tiles=True)
     H.nnz_blocks = 901                                       # another store
     best, table = autotune.tune_spmm(H, 64, timer=timer)
-    assert best == ("tiles", 256, 5) and H.use_tiles and applied[-1] == (256, 5) and len(table) == 6
+    assert best == ("tiles", 256, 5, 1) and H.use_tiles and len(table) == 7
+    assert H.spmm_cfg[(32, 64)] == best
     autotune._cache.clear()
 
 
-def test_launch_shape_hook_accepts_documented_shapes_only():
+def test_launch_hooks_accept_documented_settings_only():
     from inching_b200 import _native, autotune
     for t, b in ((256, 5), (512, 2), (1024, 1), (0, 4)):
-        _native.spmm_tune(t, b)
+        for tr in (0, 1, 2):
+            _native.spmm_tune(t, b, tr)
     with pytest.raises(AssertionError):
         _native.spmm_tune(300, 5)
+    with pytest.raises(AssertionError):
+        _native.spmm_tune(256, 5, 3)
+    _native.spmm_band_tune(64)
+    _native.spmm_band_tune(128)
+    with pytest.raises(AssertionError):
+        _native.spmm_band_tune(96)
     autotune.reset()
     assert autotune._cache == {}
