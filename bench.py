@@ -35,8 +35,13 @@ ROOT = os.path.dirname(os.path.abspath(__file__))
 sys.path.insert(0, ROOT)
 
 METRIC = "time-to-k-modes (s) at resid <=1e-6||H||"
+# From ncu captures of the 64-column FP32 pair-kernel launch on the 100k-atom assembly
+# (the files under profiles/ named below hold the command and the figures).
 TRAFFIC_B64_BYTES = 311_794_176
 TRAFFIC_B64_RATIO = 0.979
+TRAFFIC_SOURCE = "profiles/spmm_f32_b64_assembly100k.md"
+LIMITER_FRAC = 0.793
+LIMITER_SOURCE = "profiles/spmm_f32_b64_assembly100k_memory.md"
 UNIT = "s"
 
 
@@ -51,6 +56,10 @@ def parse():
     ap.add_argument("--tol", type=float, default=1e-6)
     ap.add_argument("--no-plain", action="store_true", help="skip the plain FP64 JDM comparison")
     ap.add_argument("--no-cpu", action="store_true", help="skip the CPU baseline leg")
+    ap.add_argument("--no-largest", action="store_true",
+                    help="skip the single measured solve of the largest configuration (cube2400k)")
+    ap.add_argument("--no-largest-plain", action="store_true",
+                    help="skip the plain FP64 solve of the largest configuration")
     ap.add_argument("--cpu-budget", type=float, default=15.0)
     ap.add_argument("--kernel-only", default=None, choices=["spmm32", "spmm64"],
                     help="profiling aid: build the workload's store and run only the SpMM")
@@ -231,7 +240,7 @@ def run_ours(args):
     achieved = sp["bytes"] / (sp["ms"] / 1e3) / 1e9 if sp["ms"] > 0 else None
 
     # ---- accuracy and plain FP64 comparison (one GPU only; replicas skip them) -----
-    eig_rel, t_f64_tight, plain = None, None, None
+    eig_rel, t_f64_tight, plain, cert_jdm = None, None, None, None
     if world == 1:
         from inching_b200 import graph
         from inching_b200.deflation import rigid_body_basis
@@ -247,6 +256,21 @@ def run_ours(args):
         ev = evals.double().cpu().numpy() + 1.0
         rv = ref_ev.cpu().numpy()
         eig_rel = float(np.max(np.abs(ev - rv) / np.abs(rv)))
+        # independent certificate: the reference's own algorithm (single-vector
+        # Jacobi-Davidson, FP64, Hotelling deflation) at residual <= 1e-9 ||H||
+        from inching_b200.solvers.jdm import jdm
+        torch.cuda.synchronize()
+        t0 = time.perf_counter()
+        cev, _, cinfo = jdm(H, k=k, tol=1e-9 * ref_info["normH"], Q=Q, shift=10.0, maxiter=200000,
+                            return_info=True)
+        torch.cuda.synchronize()
+        t_cert = time.perf_counter() - t0
+        cv = cev.cpu().numpy()
+        cert_jdm = {"solver": "JDM (reference algorithm), FP64, single-vector, residual <= 1e-9*||H||",
+                    "seconds": round(t_cert, 2), "outer_iterations": cinfo["iterations"],
+                    "converged": cinfo["converged"],
+                    "max_eig_rel_err_ours_vs_this": float(np.max(np.abs(ev - cv) / np.abs(cv))),
+                    "max_eig_rel_diff_f64_block_vs_this": float(np.max(np.abs(rv - cv) / np.abs(cv)))}
         if not args.no_plain:
             from inching_b200.solvers.jdm import jdm
             normH = info["normH"]
@@ -293,6 +317,15 @@ def run_ours(args):
                           f"{r['solve_sample_s']:.1f} s, projected to the {plain['outer_iterations']} iterations "
                           f"the same algorithm needed on the GPU")}
 
+    largest = None
+    if world == 1 and not args.no_largest:
+        # the largest configuration needs ~160 GB: release the headline's blocks first
+        del evals, modes
+        import gc
+        gc.collect()
+        torch.cuda.empty_cache()
+        largest = largest_entry(args, plain=not args.no_largest_plain)
+
     if world > 1:
         dist.destroy_process_group()
     if rank != 0:
@@ -311,7 +344,8 @@ def run_ours(args):
                    "mean_degree": round(info["mean_degree"], 2), "nnz_blocks": info["nnz_blocks"]},
         "accuracy": {"max_rel_residual": info["max_rel_residual"], "max_eig_rel_err_vs_f64_certificate": eig_rel,
                      "certificate": None if t_f64_tight is None else
-                     f"FP64 block solver at residual 1e-10*||H|| ({t_f64_tight:.2f} s)"},
+                     f"FP64 block solver at residual 1e-10*||H|| ({t_f64_tight:.2f} s)",
+                     "independent_certificate": cert_jdm},
         "plain_f64": plain,
         "e2e": {"value": round(e2e, 4), "unit": UNIT, "h2d_bytes_per_step": int(h2d), "d2h_bytes_per_step": int(d2h)},
         "roofline": {"bound": "hbm", "achieved": round(achieved, 1) if achieved else None, "peak": hbm,
@@ -319,17 +353,19 @@ def run_ours(args):
                      "peak_kind": peak_kind, "kernel": "FP32 SpMM (k_spmm_cols / k_spmm)",
                      "spmm_calls": sp["calls"], "spmm_ms": round(sp["ms"], 2),
                      # ncu dram__bytes_read.sum + dram__bytes_write.sum of one 64-column FP32 launch on this
-                     # workload (profiles/spmm_f32_b64_assembly100k.md): 311.8 MB against 318.6 MB algorithmic
+                     # workload: not measured by this run, copied from the profile named in traffic_source
                      "traffic": TRAFFIC_B64_BYTES, "traffic_unit": "bytes per 64-column launch",
-                     "traffic_over_algorithmic": TRAFFIC_B64_RATIO,
-                     # what bounds the kernel instead of HBM, from the ncu memory capture of the same
-                     # launch (profiles/spmm_f32_b64_assembly100k_memory.md); not measured by this run
-                     "limiter": {"unit": "L1/TEX data pipe (X_j gathers)", "throughput_frac": 0.793,
-                                 "source": "ncu capture, 64-column FP32 launch on this workload"}},
+                     "traffic_over_algorithmic": TRAFFIC_B64_RATIO, "traffic_source": TRAFFIC_SOURCE,
+                     "traffic_measured_in_this_run": False,
+                     # what bounds the kernel instead of HBM, from an ncu memory capture of the same
+                     # launch; not measured by this run
+                     "limiter": {"unit": "L1/TEX data pipe (X_j gathers)", "throughput_frac": LIMITER_FRAC,
+                                 "source": LIMITER_SOURCE, "measured_in_this_run": False}},
         "cpu_baseline": cpu,
         "clocks": clk.summary(),
         "gpu_launches": int(launches),
         "solver_info": {kk: info[kk] for kk in ("iterations", "n_spmm_filter", "n_rr", "block", "degree")},
+        "largest_config": largest,
     }
     print(json.dumps(line))
 
@@ -390,46 +426,85 @@ def run_batched(args):
         dist.destroy_process_group()
 
 
-def run_largest(args):
-    """The largest configuration: ~2.4M atoms (300 touching globules of 8,000 atoms),
-    lowest 1,000 non-rigid modes, memory-lean block solver (mixed precision, bead
-    warm start).  One step; the FP64 comparison (same algorithm, FP64 filter, no
-    warm start) only with --plain-lean."""
+def largest_solve(precision, warm, k, tol, degree=None, profile=False):
+    """One solve of the largest configuration (cube2400k: ~2.4M atoms, 300 touching
+    globules of 8,000, 7.2M dof) from device-resident coordinates: Cuthill-McKee,
+    Hessian store, rigid-body basis, bead warm start (if warm), memory-lean block
+    solver.  CUDA-event timed; returns (seconds, eigenvalues, info)."""
     import torch
     from inching_b200 import graph, synth
     from inching_b200.deflation import rigid_body_basis
     from inching_b200.hessian import HessianStore
     from inching_b200.solvers.chfsi import chfsi_lean, default_guard
     from inching_b200.warmstart import coarse_warm_start
-    k = 1000 if args.k == 256 else args.k
     Xd = torch.from_numpy(synth.workload("cube2400k") / 10.0).cuda()
+    torch.cuda.synchronize()
+    ev_ = [torch.cuda.Event(enable_timing=True) for _ in range(5)]
+    ev_[0].record()
+    order, undo = graph.cuthill_mckee(Xd, 8.0)
+    Xr = Xd[order]
+    ev_[1].record()
+    H = HessianStore(Xr, 8.0, 1.0, precisions=("f64", "f32") if precision == "mixed" else ("f64",))
+    Q = rigid_body_basis(Xr)
+    ev_[2].record()
+    # all k + guard bead modes converged: with only the k wanted ones (guard left as
+    # coarse Ritz vectors) the fine solve took 5 iterations and 96 s instead of 4 and 93 s
+    X0 = coarse_warm_start(Xr, k + default_guard(k)) if warm else None
+    ev_[3].record()
+    ev, V, info = chfsi_lean(H, k, tol=tol, Q=Q, precision=precision, X0=X0, return_info=True, degree=degree,
+                             profile=profile)
+    del X0
+    ev_[4].record()
+    torch.cuda.synchronize()
+    info["outer_ms"] = {nm: round(ev_[i].elapsed_time(ev_[i + 1]), 1)
+                        for i, nm in enumerate(("order", "hessian", "warm_start", "solve"))}
+    info["n_atoms"] = int(Xd.shape[0])
+    info["nnz_blocks"] = H.nnz_blocks
+    del V, H, Q, Xr, Xd
+    torch.cuda.empty_cache()
+    return ev_[0].elapsed_time(ev_[4]) / 1e3, ev.cpu(), info
 
-    def solve(precision, warm):
-        torch.cuda.synchronize()
-        ev_ = [torch.cuda.Event(enable_timing=True) for _ in range(5)]
-        ev_[0].record()
-        order, undo = graph.cuthill_mckee(Xd, 8.0)
-        Xr = Xd[order]
-        ev_[1].record()
-        H = HessianStore(Xr, 8.0, 1.0, precisions=("f64", "f32") if precision == "mixed" else ("f64",))
-        Q = rigid_body_basis(Xr)
-        ev_[2].record()
-        # all k + guard bead modes converged: with only the k wanted ones (guard left as
-        # coarse Ritz vectors) the fine solve took 5 iterations and 96 s instead of 4 and 93 s
-        X0 = coarse_warm_start(Xr, k + default_guard(k)) if warm else None
-        ev_[3].record()
-        ev, V, info = chfsi_lean(H, k, tol=args.tol, Q=Q, precision=precision, X0=X0, return_info=True,
-                                 degree=args.degree, profile=args.profile)
-        del X0
-        ev_[4].record()
-        torch.cuda.synchronize()
-        info["outer_ms"] = {nm: round(ev_[i].elapsed_time(ev_[i + 1]), 1)
-                            for i, nm in enumerate(("order", "hessian", "warm_start", "solve"))}
-        return ev_[0].elapsed_time(ev_[4]) / 1e3, ev, info
 
+def largest_entry(args, plain=True):
+    """The largest configuration measured once in this run (mixed precision + bead
+    warm start), and the same block algorithm in plain FP64 from a random start on
+    the same GPU, with the eigenvalue agreement between them."""
+    import numpy as np
+    import torch
+    k = 1000
+    torch.cuda.reset_peak_memory_stats()
+    with Clocks(int(os.environ.get("LOCAL_RANK", "0"))) as clk:
+        t, ev, info = largest_solve("mixed", True, k, args.tol, degree=args.degree, profile=True)
+    out = {"workload": "cube2400k: 2,400,000 atoms (300 touching globules of 8,000 in a cube), 7.2M dof, "
+                       f"cutoff 8 A, gamma 1, lowest {k} non-rigid modes, residual <= {args.tol:g}*||H||",
+           "solver": "memory-lean block Chebyshev-filtered subspace iteration, FP32 SpMM filter, FP64 "
+                     "Rayleigh-Ritz, bead-model warm start",
+           "seconds": round(t, 2), "timing": "one solve, CUDA events, coordinates resident in HBM",
+           "steps": 1, "max_rel_residual": info["max_rel_residual"], "iterations": info["iterations"],
+           "degree": info["degree"], "nnz_blocks": info["nnz_blocks"], "phases_ms": info.get("phases_ms"),
+           "outer_ms": info.get("outer_ms"), "peak_mem_gb": round(torch.cuda.max_memory_allocated() / 1e9, 1),
+           "clocks": clk.summary()}
+    if plain:
+        with Clocks(int(os.environ.get("LOCAL_RANK", "0"))) as clk2:
+            tp, evp, infop = largest_solve("f64", False, k, args.tol)
+        a, b = ev.double().numpy(), evp.double().numpy()
+        out["plain_f64"] = {"solver": "the same block algorithm in FP64 (FP64 SpMM filter), random start",
+                            "seconds": round(tp, 2), "iterations": infop["iterations"],
+                            "max_rel_residual": infop["max_rel_residual"],
+                            "speedup_mixed_warm_over_plain_f64": round(tp / t, 2),
+                            "max_eig_rel_diff_vs_mixed": float(np.max(np.abs(a - b) / np.abs(b))),
+                            "clocks": clk2.summary()}
+    return out
+
+
+def run_largest(args):
+    """The largest configuration alone: one mixed + warm solve (and with --plain-lean
+    the FP64 comparison), printed as its own line."""
+    k = 1000 if args.k == 256 else args.k
     with Clocks(0) as clk:
-        t, ev, info = solve("mixed", True)
-    line = {"metric": f"time-to-k-modes (s) at resid <=1e-6||H||", "value": round(t, 2), "unit": "s", "n_gpus": 1,
+        t, ev, info = largest_solve("mixed", True, k, args.tol, degree=args.degree, profile=args.profile)
+    import torch
+    line = {"metric": METRIC, "value": round(t, 2), "unit": "s", "n_gpus": 1,
             "steps": 1, "warmup": 0, "higher_is_better": False,
             "config": {"workload": "cube2400k: 2,400,000 atoms (300 touching globules of 8,000), 7.2M dof, "
                                    f"lowest {k} non-rigid modes", "solver": "memory-lean block ChFSI, mixed + warm"},
@@ -437,8 +512,7 @@ def run_largest(args):
             "phases_ms": info.get("phases_ms"), "outer_ms": info.get("outer_ms"),
             "peak_mem_gb": round(torch.cuda.max_memory_allocated() / 1e9, 1), "clocks": clk.summary()}
     if args.plain_lean:
-        del ev
-        tp, evp, infop = solve("f64", False)
+        tp, evp, infop = largest_solve("f64", False, k, args.tol)
         line["plain_f64_block"] = {"seconds": round(tp, 2), "iterations": infop["iterations"],
                                    "max_rel_residual": infop["max_rel_residual"]}
     print(json.dumps(line))
@@ -512,24 +586,39 @@ def run_shell(args):
     print(json.dumps(line))
 
 
+# Outer Jacobi-Davidson iterations the reference algorithm (FP64, single vector,
+# Hotelling deflation) needs for all k modes at residual <= 1e-6*||H|| on these
+# workloads: counted on the B200 by the plain_f64 leg of this benchmark (the GPU run
+# of the identical algorithm; 869 on assembly100k with k = 256).  The reference arm
+# projects its CPU per-iteration time to this count.
+PLAIN_JDM_ITERATIONS = {("assembly100k", 256): 869}
+
+
 def run_reference(args):
     """Reference arm: the reference path's CPU restatement (the reference's own
     solvers need CuPy and cannot run on the CPU), timed on the host cores on the
-    same workload and metric; rank 0 only."""
+    same workload and metric; rank 0 only.  Each step runs the preprocessing in
+    full and a bounded Jacobi-Davidson sample; the step's value is the projection
+    of the full solve (preprocessing + per-iteration time x the iteration count
+    the identical algorithm needs), labelled as such, with the measured lower bound
+    beside it."""
     rank = int(os.environ.get("RANK", "0"))
     if rank != 0:
         return
     from inching_b200 import synth
     from oracle.baseline import cpu_time_to_modes
     Xh = synth.workload(args.workload) / 10.0
-    vals = []
+    iters = PLAIN_JDM_ITERATIONS.get((args.workload, args.k))
+    budget = min(args.cpu_budget, 8.0)
+    for _ in range(min(args.warmup, 1)):
+        cpu_time_to_modes(Xh, args.k, budget_s=1.0, tol_rel=args.tol)
+    proj, low = [], []
     r = None
     for _ in range(max(args.steps, 1)):
-        r = cpu_time_to_modes(Xh, args.k, budget_s=args.cpu_budget, tol_rel=args.tol)
-        # per-iteration rate of the JDM restatement; without the GPU iteration count the
-        # projection uses the sample's own rate over the modes converged so far
-        vals.append(r["preprocess_s"] + r["solve_sample_s"])
-    v = sum(vals) / len(vals)
+        r = cpu_time_to_modes(Xh, args.k, budget_s=budget, tol_rel=args.tol, plain_iterations=iters)
+        low.append(r["preprocess_s"] + r["solve_sample_s"])
+        proj.append(r.get("projected_s", low[-1]))
+    v = sum(proj) / len(proj)
     arpack = None
     if Xh.shape[0] <= 20000:
         # the reference's own CPU baseline (ARPACK on the symmetrised Hessian), feasible in
@@ -538,12 +627,21 @@ def run_reference(args):
         t_arp, _ = arpack_time_to_modes(Xh, args.k)
         arpack = {"seconds": round(t_arp, 3), "call": "scipy.sparse.linalg.eigsh(which='SA'), k + 6 modes, "
                                                       "no deflation, full solve"}
+    if iters is not None:
+        sample = (f"CPU restatement of the reference path: cKDTree neighbours + sequential Cuthill-McKee + FP64 "
+                  f"Hessian in full ({r['preprocess_s']:.1f} s), then {r['sample_iterations']} outer JDM iterations "
+                  f"in {r['solve_sample_s']:.1f} s, PROJECTED to the {iters} iterations the identical algorithm "
+                  f"needs on this workload")
+    else:
+        sample = (f"CPU restatement: preprocessing in full + {budget:.0f} s of JDM "
+                  f"({r['sample_iterations']} outer iterations); a LOWER BOUND of the full solve")
     line = {"impl": "reference", "metric": METRIC, "value": round(v, 3), "unit": UNIT, "n_gpus": 1,
             "steps": args.steps, "warmup": args.warmup, "higher_is_better": False,
             "config": {"workload": args.workload, "k": args.k},
+            "value_kind": "projection of the full solve" if iters is not None else "lower bound",
+            "measured_lower_bound_s": round(sum(low) / len(low), 3),
             "cpu_baseline": {"value": round(v, 3), "unit": UNIT, "cores": r["cores"], "kind": "port",
-                             "sample": f"CPU restatement: preprocessing in full + {args.cpu_budget:.0f} s of JDM "
-                                       f"({r['sample_iterations']} outer iterations); a lower bound of the full solve"},
+                             "sample": sample},
             "e2e": {"value": round(v, 3), "unit": UNIT, "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0}}
     if arpack is not None:
         line["arpack"] = arpack

@@ -474,16 +474,20 @@ def lean_degree(A, p):
 
 
 def chfsi_lean(A, k, tol=1e-6, Q=None, precision="mixed", degree=None, guard=None, maxiter=100, X0=None, seed=0,
-               chunk=256, row_chunk=1 << 20, window=512, verbose=False, return_info=False, profile=False):
+               chunk=256, row_chunk=1 << 20, window=512, verbose=False, return_info=False, profile=False,
+               fold_orth=True):
     """Same iteration as chfsi() with one (n, p) FP64 array B holding the locked
     modes (columns [0, L)) and the active block (columns [L, p)):
 
       * the filter runs on column chunks of `chunk` vectors (it acts column by
         column), with FP32 (or FP64) buffers of that width only;
-      * Rayleigh-Ritz forms G = Y^T H Y chunk by chunk from an FP64 product, so
-        H Y is never stored; explicit FP64 residuals are taken for the leading
-        `window` wanted active columns, the only ones that can lock next;
-      * rotations, projections and Cholesky-QR update B in row chunks;
+      * Rayleigh-Ritz forms G = Y^T H Y chunk by chunk (H Y on the FP32 store in
+        mixed precision, FP64 otherwise), so H Y is never stored; explicit FP64
+        residuals are taken for the leading `window` wanted active columns, the
+        only ones that can lock next;
+      * rotations, projections and Cholesky-QR update B in row chunks; with
+        fold_orth (default) the second Cholesky-QR pass's factor is folded into
+        the Rayleigh-Ritz rotation (see orth());
       * converged leading active columns become locked by moving L.
     Peak memory is about n*p*8 bytes plus a few (n, chunk) buffers: the 2.4M-atom,
     1000-mode configuration (n = 7.2M, p = 1250) needs ~72 GB for B.  A contiguous
@@ -529,21 +533,39 @@ def chfsi_lean(A, k, tol=1e-6, Q=None, precision="mixed", degree=None, guard=Non
                 for rs in _rows(n, row_chunk):
                     B[rs, act] -= basis[rs] @ C
 
-    def orth(L):
-        act = slice(L, p)
-        for _ in range(2):
-            G = B[:, act].t() @ B[:, act]
-            R, info = torch.linalg.cholesky_ex(G, upper=True)
-            if int(info) != 0:
-                raise RuntimeError("chfsi_lean: Gram matrix not positive definite")
-            Rinv = torch.linalg.solve_triangular(R, torch.eye(R.shape[0], dtype=R.dtype, device=dev), upper=True)
-            for rs in _rows(n, row_chunk):
-                B[rs, act] = B[rs, act] @ Rinv
+    def orth_f64_pass(act):
+        G = B[:, act].t() @ B[:, act]
+        R, info = torch.linalg.cholesky_ex(G, upper=True)
+        if int(info) != 0:
+            raise RuntimeError("chfsi_lean: Gram matrix not positive definite")
+        Rinv = torch.linalg.solve_triangular(R, torch.eye(R.shape[0], dtype=R.dtype, device=dev), upper=True)
+        for rs in _rows(n, row_chunk):
+            B[rs, act] = B[rs, act] @ Rinv
 
-    def rayleigh_ritz(L):
+    def orth(L):
+        """Cholesky-QR of the active block.  With fold_orth, one FP64 pass (Gram,
+        Cholesky, rotation) and then the second pass's FP64 Gram only: its factor
+        R2 is returned instead of applied, and the Rayleigh-Ritz step folds R2^-1
+        into its rotation (one tall rotation fewer per iteration).  Returns R2, or
+        None when the block is left orthonormal (two full passes)."""
+        act = slice(L, p)
+        orth_f64_pass(act)
+        if not fold_orth:
+            orth_f64_pass(act)
+            return None
+        G2 = B[:, act].t() @ B[:, act]
+        R2, info = torch.linalg.cholesky_ex(G2, upper=True)
+        if int(info) != 0:
+            raise RuntimeError("chfsi_lean: Gram matrix not positive definite")
+        return R2
+
+    def rayleigh_ritz(L, R2=None):
         """Rotate the active block to Ritz vectors; returns (theta, residual norms).
         Explicit FP64 residuals are computed for the leading `window` wanted active
-        columns only (locking proceeds from the front); the others report inf."""
+        columns only (locking proceeds from the front); the others report inf.
+        With R2 (upper triangular) the active block Y is not orthonormal but Y R2^-1
+        is: the projected matrix becomes R2^-T (Y^T H Y) R2^-1 and the rotation
+        R2^-1 W."""
         act_n = p - L
         G = torch.zeros((act_n, act_n), dtype=torch.float64, device=dev)
         for cs in range(L, p, chunk):
@@ -559,8 +581,14 @@ def chfsi_lean(A, k, tol=1e-6, Q=None, precision="mixed", degree=None, guard=Non
                 G[:, cs - L:ce - L] = B[:, L:].t() @ HYc
             del HYc
         G = 0.5 * (G + G.t())
+        if R2 is not None:
+            Rinv = torch.linalg.solve_triangular(R2, torch.eye(R2.shape[0], dtype=R2.dtype, device=dev), upper=True)
+            G = Rinv.t() @ G @ Rinv
+            G = 0.5 * (G + G.t())
         with ph("rr_eigh"):
             th, Wd = eigh_sym(G)
+        if R2 is not None:
+            Wd = Rinv @ Wd
         with ph("rr_rotate"):
             for rs in _rows(n, row_chunk):
                 B[rs, L:] = B[rs, L:] @ Wd
@@ -579,9 +607,9 @@ def chfsi_lean(A, k, tol=1e-6, Q=None, precision="mixed", degree=None, guard=Non
     with ph("project"):
         project(0)
     with ph("orth"):
-        orth(0)
+        R2 = orth(0)
     with ph("rr"):
-        th, res = rayleigh_ritz(0)
+        th, res = rayleigh_ritz(0, R2)
     L = 0
     locked_theta = []
     filt = _Filter(A, prec)
@@ -622,9 +650,9 @@ def chfsi_lean(A, k, tol=1e-6, Q=None, precision="mixed", degree=None, guard=Non
         with ph("project"):
             project(L)
         with ph("orth"):
-            orth(L)
+            R2 = orth(L)
         with ph("rr"):
-            th, res = rayleigh_ritz(L)
+            th, res = rayleigh_ritz(L, R2)
     converged = L >= k
     # final FP64 Rayleigh-Ritz over the first k columns, explicit residuals
     ph_final = ph("final_f64")

@@ -159,18 +159,20 @@ def test_block_solver_returns_whole_orthonormal_block(dense, maxiter):
         assert np.abs(S.numpy() - w[6:26]).max() < 1e-8 * w[-1]
 
 
-@pytest.mark.parametrize("precision,tol", [("f64", 1e-9), ("mixed", 1e-6)])
-def test_lean_block_solver_chunked_paths_on_dense_double(dense, precision, tol):
+@pytest.mark.parametrize("precision,tol,fold", [("f64", 1e-9, True), ("mixed", 1e-6, True), ("mixed", 1e-6, False)])
+def test_lean_block_solver_chunked_paths_on_dense_double(dense, precision, tol, fold):
     """chfsi_lean with chunks smaller than the block (column chunks of the filter,
     row chunks of rotations and projections, a residual window shorter than the
     wanted count), and with a caller's FP64 block X0 of the full width taken over
-    in place: the eigenvalues of the dense Hessian, orthonormal vectors."""
+    in place: the eigenvalues of the dense Hessian, orthonormal vectors; with the
+    second Cholesky-QR pass's factor folded into the Rayleigh-Ritz rotation and
+    with two full passes."""
     from inching_b200.solvers.chfsi import chfsi_lean, default_guard
     w = dense["w"]
     n, k = dense["F"].shape[0], 20
     X0 = torch.randn((n, k + default_guard(k)), generator=torch.Generator().manual_seed(1), dtype=torch.float64)
     S, V, info = chfsi_lean(dense["F"], k, tol=tol, Q=dense["Q"], precision=precision, chunk=16, row_chunk=256,
-                            window=12, X0=X0, return_info=True)
+                            window=12, X0=X0, return_info=True, fold_orth=fold)
     assert info["converged"] and info["max_rel_residual"] <= 1.5 * tol
     assert np.abs(S.numpy() - w[6:26]).max() < (1e-8 if precision == "f64" else 1e-4) * w[-1]
     assert (V.t() @ V - torch.eye(k, dtype=V.dtype)).abs().max() < 1e-10
