@@ -56,6 +56,8 @@ def parse():
     ap.add_argument("--tol", type=float, default=1e-6)
     ap.add_argument("--no-plain", action="store_true", help="skip the plain FP64 JDM comparison")
     ap.add_argument("--no-cpu", action="store_true", help="skip the CPU baseline leg")
+    ap.add_argument("--no-cert", action="store_true", help="skip the accuracy certificates (profiling aid)")
+    ap.add_argument("--no-e2e", action="store_true", help="skip the end-to-end leg (profiling aid)")
     ap.add_argument("--no-largest", action="store_true",
                     help="skip the single measured solve of the largest configuration (cube2400k)")
     ap.add_argument("--no-largest-plain", action="store_true",
@@ -241,7 +243,7 @@ def run_ours(args):
 
     # ---- accuracy and plain FP64 comparison (one GPU only; replicas skip them) -----
     eig_rel, t_f64_tight, plain, cert_jdm = None, None, None, None
-    if world == 1:
+    if world == 1 and not args.no_cert:
         from inching_b200 import graph
         from inching_b200.deflation import rigid_body_basis
         from inching_b200.hessian import HessianStore
@@ -291,19 +293,22 @@ def run_ours(args):
     # ---- end to end through the public host API -----------------------------------
     # untimed warm-up in the timed loop's own pattern (the previous result is still held
     # while the next call runs, so the pinned host cache reaches its steady state)
-    ev_h, modes_h, info_h = normal_modes(Xh, k, solver="chfsi", precision="mixed", tol=tol, warm_start="coarse")
-    ev_h, modes_h, info_h = normal_modes(Xh, k, solver="chfsi", precision="mixed", tol=tol, warm_start="coarse")
     e2e_times = []
-    for _ in range(args.steps):
+    if not args.no_e2e:
+        ev_h, modes_h, info_h = normal_modes(Xh, k, solver="chfsi", precision="mixed", tol=tol,
+                                             warm_start="coarse")
+        ev_h, modes_h, info_h = normal_modes(Xh, k, solver="chfsi", precision="mixed", tol=tol,
+                                             warm_start="coarse")
+    for _ in range(0 if args.no_e2e else args.steps):
         flush_l2(l2)
         torch.cuda.synchronize()
         t0 = time.perf_counter()
         ev_h, modes_h, info_h = normal_modes(Xh, k, solver="chfsi", precision="mixed", tol=tol,
                                              warm_start="coarse")
         e2e_times.append(time.perf_counter() - t0)
-    e2e = replicas.max_over_ranks(sum(e2e_times) / len(e2e_times))
+    e2e = replicas.max_over_ranks(sum(e2e_times) / len(e2e_times)) if e2e_times else None
     h2d = Xh.size * 8
-    d2h = ev_h.size * 8 + modes_h.size * 8
+    d2h = (ev_h.size * 8 + modes_h.size * 8) if e2e_times else None
 
     # ---- CPU baseline (rank 0, one GPU only) --------------------------------------
     cpu = None
@@ -347,7 +352,8 @@ def run_ours(args):
                      f"FP64 block solver at residual 1e-10*||H|| ({t_f64_tight:.2f} s)",
                      "independent_certificate": cert_jdm},
         "plain_f64": plain,
-        "e2e": {"value": round(e2e, 4), "unit": UNIT, "h2d_bytes_per_step": int(h2d), "d2h_bytes_per_step": int(d2h)},
+        "e2e": None if e2e is None else {"value": round(e2e, 4), "unit": UNIT, "h2d_bytes_per_step": int(h2d),
+                                         "d2h_bytes_per_step": int(d2h)},
         "roofline": {"bound": "hbm", "achieved": round(achieved, 1) if achieved else None, "peak": hbm,
                      "unit": "GB/s", "frac": round(achieved / hbm, 4) if achieved else None,
                      "peak_kind": peak_kind, "kernel": "FP32 SpMM (k_spmm_cols / k_spmm)",
