@@ -367,7 +367,7 @@ def spmm(prec, n_atoms, rowptr, ent, diag, X, Y, *, alpha=1.0, gamma=0.0, beta=0
                       _stream()))
     tiles = 0
     rem = b
-    for t in ((64, 32, 16, 8, 4, 2, 1) if prec == 32 else (32, 16, 8, 4, 2, 1)):
+    for t in ((128, 64, 32, 16, 8, 4, 2, 1) if prec == 32 else (32, 16, 8, 4, 2, 1)):
         while rem >= t:
             rem -= t
             tiles += 1

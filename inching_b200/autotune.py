@@ -28,7 +28,8 @@ _cache = {}
 
 
 def _width_class(b):
-    return 64 if b >= 64 else (32 if b >= 32 else (8 if b >= 8 else b))
+    from .hessian import width_class
+    return width_class(b)
 
 
 def _apply(H, cfg):

@@ -181,6 +181,10 @@ struct VecT<double, 1> {
   using t = double;
 };
 template <>
+struct VecT<float, 4> {
+  using t = float4;
+};
+template <>
 struct VecT<double, 2> {
   using t = double2;
 };
@@ -189,6 +193,12 @@ template <class T, int V>
 __device__ __forceinline__ void vld(const T* p, T (&x)[V]) {
   if constexpr (V == 1) {
     x[0] = __ldg(p);
+  } else if constexpr (V == 4) {
+    const float4 v = __ldg(reinterpret_cast<const float4*>(p));
+    x[0] = v.x;
+    x[1] = v.y;
+    x[2] = v.z;
+    x[3] = v.w;
   } else {
     const typename VecT<T, 2>::t v = __ldg(reinterpret_cast<const typename VecT<T, 2>::t*>(p));
     x[0] = v.x;
@@ -218,7 +228,9 @@ __device__ __forceinline__ void cols_row(int64_t i, const int64_t* __restrict__ 
     for (int v = 0; v < V; ++v) acc[0][t][v] = acc[1][t][v] = acc[2][t][v] = T(0);
   const int64_t e1 = rowptr[i + 1];
   const T* Xc = X + c0 + cl * V;
-#pragma unroll 2
+  // 128-column rows (float4 gathers) keep four entries' loads in flight
+  constexpr int kUnrollE = B >= 128 ? 4 : 2;
+#pragma unroll kUnrollE
   for (int64_t e = rowptr[i]; e < e1; ++e) {
     T wx, wy, wz;
     int j;
@@ -511,7 +523,11 @@ cudaError_t launch_tile(int64_t n_atoms, const int64_t* rowptr, const void* ent,
 #define COLS_LAUNCH(NTV)                                                                                     \
   {                                                                                                           \
     const int blocks = grid_for(n_atoms, 4 * NTV / 32, 148 * bps);                                            \
-    if (vec)                                                                                                  \
+    if constexpr (B == 128 && sizeof(T) == 4) {                                                               \
+      k_spmm_cols<T, B, 4, NTV><<<blocks, NTV, 0, stream>>>(n_atoms, rowptr, ent, diag, X, ldx, Y, ldy, Yin,   \
+                                                            ldyin, Acc, ldacc, c0, ep, Q, ndof, coef,        \
+                                                            row_counter, trav);                              \
+    } else if (vec)                                                                                           \
       k_spmm_cols<T, B, 2, NTV><<<blocks, NTV, 0, stream>>>(n_atoms, rowptr, ent, diag, X, ldx, Y, ldy, Yin,   \
                                                             ldyin, Acc, ldacc, c0, ep, Q, ndof, coef,        \
                                                             row_counter, trav);                              \
@@ -567,7 +583,14 @@ cudaError_t run(int64_t n_atoms, const int64_t* rowptr, const void* ent, const v
   c0 += BB;
     bool done64 = false;
     if constexpr (sizeof(T) == 4) {
-      if (rem >= 64) {
+      // 128-column tiles gather float4 rows: every vector row 16-byte aligned
+      const bool al16 = (ldx % 4 == 0) && (ldy % 4 == 0) && (c0 % 4 == 0) && ((uintptr_t)X % 16 == 0) &&
+                        ((uintptr_t)Y % 16 == 0) && (!ep.has_yin || ((ldyin % 4 == 0) && ((uintptr_t)Yin % 16 == 0))) &&
+                        (!ep.accumulate || ((ldacc % 4 == 0) && ((uintptr_t)Acc % 16 == 0)));
+      if (rem >= 128 && al16) {
+        TILE(128, 0)
+        done64 = true;
+      } else if (rem >= 64) {
         TILE(64, 0)
         done64 = true;
       }
@@ -613,9 +636,9 @@ extern "C" size_t inch_spmm_workspace_size(int64_t n_atoms, int32_t b, int32_t r
   (void)n_atoms;
   (void)b;
   Sizer s;
-  s.take<int>(1);                              // row counter of the wide-block kernel
-  s.take<double>((size_t)kQxBlocks * 8 * 64);  // partial sums (r <= 8, tile <= 64)
-  s.take<double>(8 * 64);                      // coefficients
+  s.take<int>(1);                               // row counter of the wide-block kernel
+  s.take<double>((size_t)kQxBlocks * 8 * 128);  // partial sums (r <= 8, tile <= 128)
+  s.take<double>(8 * 128);                      // coefficients
   (void)r;
   return s.bytes();
 }
@@ -627,7 +650,8 @@ extern "C" inch_status inch_spmm(int32_t prec, int64_t n_atoms, const int64_t* r
   INCH_REQUIRE(prec == 32 || prec == 64, INCH_INVALID_ARG, "inch_spmm: prec must be 32 or 64");
   INCH_REQUIRE(rowptr && ent && diag && X && Y && ep_in, INCH_INVALID_ARG, "inch_spmm: NULL argument");
   INCH_REQUIRE(n_atoms >= 1 && n_atoms < (int64_t(1) << 31), INCH_INVALID_ARG, "inch_spmm: n_atoms out of range");
-  INCH_REQUIRE(b >= 1 && b <= 64, INCH_INVALID_ARG, "inch_spmm: b=%d outside 1..64", b);
+  INCH_REQUIRE(b >= 1 && b <= (prec == 32 ? 128 : 64), INCH_INVALID_ARG, "inch_spmm: b=%d outside 1..%d", b,
+               prec == 32 ? 128 : 64);
   INCH_REQUIRE(ldx >= b && ldy >= b, INCH_INVALID_ARG, "inch_spmm: leading dimension below b");
   INCH_REQUIRE(X != Y, INCH_INVALID_ARG, "inch_spmm: X and Y must not alias");
   const inch_spmm_epilogue& e = *ep_in;
@@ -645,8 +669,8 @@ extern "C" inch_status inch_spmm(int32_t prec, int64_t n_atoms, const int64_t* r
   if (ws != nullptr || e.r > 0) {
     Carver c(ws, ws_bytes);
     counter = c.take<int>(1);
-    partial = c.take<double>((size_t)kQxBlocks * 8 * 64);
-    coef = c.take<double>(8 * 64);
+    partial = c.take<double>((size_t)kQxBlocks * 8 * 128);
+    coef = c.take<double>(8 * 128);
     INCH_REQUIRE(c.ok, INCH_OOM, "inch_spmm: workspace of %zu bytes, need %zu", ws_bytes,
                  inch_spmm_workspace_size(n_atoms, b, e.r));
   }

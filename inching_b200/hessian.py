@@ -160,8 +160,7 @@ class HessianStore:
         if out is None:
             out = torch.empty_like(X)
         if self.spmm_cfg:
-            bw = 1 if X.dim() == 1 else X.shape[1]
-            cfg = self.spmm_cfg.get((prec, 64 if bw >= 64 else (32 if bw >= 32 else (8 if bw >= 8 else bw))))
+            cfg = self.spmm_cfg.get((prec, width_class(1 if X.dim() == 1 else X.shape[1])))
             if cfg is not None:
                 from .autotune import apply_config
                 apply_config(self, cfg)
@@ -219,11 +218,12 @@ class HessianStore:
             if kw.get("acc") is not None:
                 kw["acc"].copy_(kwp["acc"][:, :b])
             return out
-        if X.dim() == 1 or X.shape[1] <= 64:
+        panel = 128 if prec == 32 else 64       # widest call the pair kernel takes
+        if X.dim() == 1 or X.shape[1] <= panel:
             return _native.spmm(prec, self.n_atoms, self.rowptr, ent, diag, X, out, **epilogue)
-        # the kernel takes up to 64 columns per call: walk column panels
-        for c0 in range(0, X.shape[1], 64):
-            sl = slice(c0, min(c0 + 64, X.shape[1]))
+        # walk column panels
+        for c0 in range(0, X.shape[1], panel):
+            sl = slice(c0, min(c0 + panel, X.shape[1]))
             kw = dict(epilogue)
             for key in ("Yin", "acc"):
                 if kw.get(key) is not None:
@@ -281,6 +281,12 @@ class HessianStore:
         return A
 
 
+def width_class(b):
+    """Launch class of a b-column product: the kernel tile it mostly runs (128, 64,
+    32 or 8 columns; narrower products are their own class)."""
+    return 128 if b >= 128 else (64 if b >= 64 else (32 if b >= 32 else (8 if b >= 8 else b)))
+
+
 def _band_aligned(m, vec):
     """Whether a (rows, b) block can go to the band kernel as it is: its data starts
     on 16 bytes and its leading dimension is a multiple of vec elements."""
@@ -288,12 +294,13 @@ def _band_aligned(m, vec):
 
 
 def _launches(b, prec):
-    """SpMM kernel launches for b columns (tiles of 64/32/16/8/4/2/1 in FP32,
-    32/16/8/4/2/1 in FP64, per 64-column panel)."""
+    """SpMM kernel launches for b columns (tiles of 128/64/32/16/8/4/2/1 in FP32 per
+    128-column panel, 32/16/8/4/2/1 in FP64 per 64-column panel)."""
     n = 0
-    for c0 in range(0, b, 64):
-        rem = min(64, b - c0)
-        for t in ((64, 32, 16, 8, 4, 2, 1) if prec == 32 else (32, 16, 8, 4, 2, 1)):
+    panel = 128 if prec == 32 else 64
+    for c0 in range(0, b, panel):
+        rem = min(panel, b - c0)
+        for t in ((128, 64, 32, 16, 8, 4, 2, 1) if prec == 32 else (32, 16, 8, 4, 2, 1)):
             while rem >= t:
                 rem -= t
                 n += 1

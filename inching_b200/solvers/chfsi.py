@@ -51,7 +51,7 @@ def autotune_store(A, precs):
     from ..autotune import tune_spmm
     for prec in precs:
         if A.has(prec):
-            tune_spmm(A, 64, prec=prec)
+            tune_spmm(A, 128 if prec == 32 else 64, prec=prec)
 
 
 def default_guard(k):

@@ -225,8 +225,12 @@ inch_status inch_mp_adam(float* w, const float* g, float* m1, float* m2, int64_t
  * where Q is the (r, 3N) row-major FP64 deflation basis (r <= 8; explicit
  * Hotelling deflation); its coefficients Q X are reduced inside the call.
  * Yin may alias Y.  prec: 64 -> f64 store and f64 vectors; 32 -> f32 store and
- * f32 vectors.  Supported b: 1..64 at both precisions (FP64 runs 64 columns as
- * two 32-column tiles).
+ * f32 vectors.  Supported b: 1..128 in FP32 (128-column tiles with float4 gathers
+ * when every vector block is 16-byte aligned with leading dimensions and column
+ * offset multiples of 4, else 64-column tiles), 1..64 in FP64 (two 32-column
+ * tiles).  With a workspace the wide-block kernel hands out its rows from a
+ * counter in it (inch_spmm_traversal); calls that share a workspace must not
+ * overlap on the GPU.
  * ------------------------------------------------------------------------- */
 typedef struct {
   double alpha, gamma, beta, mu, hot_shift;
