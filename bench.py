@@ -35,13 +35,13 @@ ROOT = os.path.dirname(os.path.abspath(__file__))
 sys.path.insert(0, ROOT)
 
 METRIC = "time-to-k-modes (s) at resid <=1e-6||H||"
-# From ncu captures of the 64-column FP32 pair-kernel launch on the 100k-atom assembly
-# (the files under profiles/ named below hold the command and the figures).
-TRAFFIC_B64_BYTES = 311_794_176
-TRAFFIC_B64_RATIO = 0.979
-TRAFFIC_SOURCE = "profiles/spmm_f32_b64_assembly100k.md"
-LIMITER_FRAC = 0.793
-LIMITER_SOURCE = "profiles/spmm_f32_b64_assembly100k_memory.md"
+# From the ncu capture of the 128-column FP32 pair-kernel launch on the 100k-atom
+# assembly (the file under profiles/ named below holds the command and the figures).
+TRAFFIC_B128_BYTES = 456_450_304
+TRAFFIC_B128_RATIO = 0.966
+TRAFFIC_SOURCE = "profiles/spmm_f32_b128_assembly100k.md"
+LIMITER_FRAC = 0.771
+LIMITER_SOURCE = "profiles/spmm_f32_b128_assembly100k.md"
 UNIT = "s"
 
 
@@ -356,16 +356,17 @@ def run_ours(args):
                                          "d2h_bytes_per_step": int(d2h)},
         "roofline": {"bound": "hbm", "achieved": round(achieved, 1) if achieved else None, "peak": hbm,
                      "unit": "GB/s", "frac": round(achieved / hbm, 4) if achieved else None,
-                     "peak_kind": peak_kind, "kernel": "FP32 SpMM (k_spmm_cols / k_spmm)",
+                     "peak_kind": peak_kind, "kernel": "FP32 SpMM (k_spmm_cols<float, 128, 4> / k_spmm)",
                      "spmm_calls": sp["calls"], "spmm_ms": round(sp["ms"], 2),
                      # ncu dram__bytes_read.sum + dram__bytes_write.sum of one 64-column FP32 launch on this
                      # workload: not measured by this run, copied from the profile named in traffic_source
-                     "traffic": TRAFFIC_B64_BYTES, "traffic_unit": "bytes per 64-column launch",
-                     "traffic_over_algorithmic": TRAFFIC_B64_RATIO, "traffic_source": TRAFFIC_SOURCE,
+                     "traffic": TRAFFIC_B128_BYTES, "traffic_unit": "bytes per 128-column launch",
+                     "traffic_over_algorithmic": TRAFFIC_B128_RATIO, "traffic_source": TRAFFIC_SOURCE,
                      "traffic_measured_in_this_run": False,
                      # what bounds the kernel instead of HBM, from an ncu memory capture of the same
                      # launch; not measured by this run
-                     "limiter": {"unit": "L1/TEX data pipe (X_j gathers)", "throughput_frac": LIMITER_FRAC,
+                     "limiter": {"unit": "L2 throughput (X_j gathers miss L1: 6.8 % hit rate)",
+                                 "throughput_frac": LIMITER_FRAC,
                                  "source": LIMITER_SOURCE, "measured_in_this_run": False}},
         "cpu_baseline": cpu,
         "clocks": clk.summary(),
