@@ -97,6 +97,9 @@ _SIGS = {
     "inch_spmm_traversal": (ctypes.c_int, [c_int32]),
     "inch_spmm_seg": (ctypes.c_int, [c_int32, c_int64, c_void_p, c_void_p, c_void_p, c_void_p, c_int64, c_int32,
                                      c_void_p, c_int64, c_void_p, c_int64, c_void_p, c_void_p, c_void_p]),
+    "inch_spmm_seg_ws": (ctypes.c_int, [c_int32, c_int64, c_void_p, c_void_p, c_void_p, c_void_p, c_int64, c_int32,
+                                        c_void_p, c_int64, c_void_p, c_int64, c_void_p, c_void_p, c_void_p, c_size_t,
+                                        c_void_p]),
     "inch_spmm": (ctypes.c_int, [c_int32, c_int64, c_void_p, c_void_p, c_void_p, c_void_p, c_int64, c_int32,
                                  c_void_p, c_int64, c_void_p, c_int64, c_void_p, c_int64, c_void_p,
                                  POINTER(SpmmEpilogue), c_void_p, c_size_t, c_void_p]),
@@ -132,6 +135,9 @@ _SIGS = {
                                        c_int64, c_void_p, c_void_p]),
     "inch_mp_adam": (ctypes.c_int, [c_void_p, c_void_p, c_void_p, c_void_p, c_int64, ctypes.c_float,
                                     ctypes.c_float, ctypes.c_float, ctypes.c_float, c_int32, c_void_p]),
+    "inch_mp_gemm_workspace_size": (c_size_t, [c_int32, c_int32, c_int32]),
+    "inch_mp_gemm": (ctypes.c_int, [c_int32, c_int32, c_int32, c_void_p, c_int64, c_int64, c_void_p, c_int64, c_int64,
+                                    c_void_p, c_int64, ctypes.c_float, c_void_p, c_size_t, c_void_p]),
     "inch_spmm_noalloc": (ctypes.c_int, [c_int32, c_int64, c_void_p, c_void_p, c_void_p, c_void_p, c_int64,
                                          c_int32, c_void_p, c_int64, c_void_p, c_int64, c_void_p, c_int64,
                                          c_void_p, POINTER(SpmmEpilogue), c_void_p]),
@@ -309,17 +315,23 @@ _ws_cache = {}
 
 def spmm_seg(prec, n_atoms, rowptr, ent, diag, X, Y, atom_seg, seg_coef, Yin=None):
     """Y = alpha_s (H X) + gamma_s X + beta_s Yin with (alpha, gamma, beta) per segment s
-    of atom i (atom_seg int32 (N,), seg_coef float64 (S, 3)).  X, Y: (3N, b), b <= 64."""
+    of atom i (atom_seg int32 (N,), seg_coef float64 (S, 3)).  X, Y: (3N, b), b <= 128
+    (FP32) / 64 (FP64); runs with the device's cached workspace (row counter)."""
     L = lib()
     b = 1 if X.dim() == 1 else X.shape[1]
     ldx = 1 if X.dim() == 1 else X.stride(0)
     ldy = 1 if Y.dim() == 1 else Y.stride(0)
     ldyin = 0 if Yin is None else (1 if Yin.dim() == 1 else Yin.stride(0))
-    check(L.inch_spmm_seg(prec, n_atoms, _ptr(rowptr), _ptr(ent), _ptr(diag), _ptr(X), ldx, b, _ptr(Y), ldy,
-                          _ptr(Yin), ldyin, _ptr(atom_seg), _ptr(seg_coef), _stream()))
+    dev = X.device
+    ws = _ws_cache.get((dev.index, False))
+    if ws is None:
+        ws = _ws(L.inch_spmm_workspace_size(n_atoms, b, 0), dev)
+        _ws_cache[(dev.index, False)] = ws
+    check(L.inch_spmm_seg_ws(prec, n_atoms, _ptr(rowptr), _ptr(ent), _ptr(diag), _ptr(X), ldx, b, _ptr(Y), ldy,
+                             _ptr(Yin), ldyin, _ptr(atom_seg), _ptr(seg_coef), _ptr(ws), ws.numel(), _stream()))
     tiles = 0
     rem = b
-    for t in ((64, 32, 16, 8, 4, 2, 1) if prec == 32 else (32, 16, 8, 4, 2, 1)):
+    for t in ((128, 64, 32, 16, 8, 4, 2, 1) if prec == 32 else (32, 16, 8, 4, 2, 1)):
         while rem >= t:
             rem -= t
             tiles += 1
@@ -471,6 +483,32 @@ def spmm_tiles_seg(prec, n_atoms, uptr, pptr, urec, pw, diag, X, Y, atom_seg, se
 # ---------------------------------------------------------------------------
 # Message-passing network kernels (learned warm start)
 # ---------------------------------------------------------------------------
+_gemm_ws = {}
+
+
+def mp_gemm(A, B, C, beta=0.0):
+    """C = A B + beta C (FP32) with the package's dense-layer kernel; A, B may be any
+    strided 2-D views (transposes included), C row-major with unit column stride."""
+    for t, nm in ((A, "A"), (B, "B"), (C, "C")):
+        if not (isinstance(t, torch.Tensor) and t.is_cuda and t.dtype == torch.float32 and t.dim() == 2):
+            raise AssertionError(f"ABORTED. {nm} must be a 2-D float32 CUDA tensor")
+    M, K = A.shape
+    K2, N = B.shape
+    if K2 != K or tuple(C.shape) != (M, N) or C.stride(1) != 1:
+        raise AssertionError("ABORTED. mp_gemm: shapes or output layout do not match")
+    L = lib()
+    need = L.inch_mp_gemm_workspace_size(M, N, K)
+    dev = C.device.index
+    ws = _gemm_ws.get(dev)
+    if ws is None or ws.numel() < need:
+        ws = _ws(need, C.device)
+        _gemm_ws[dev] = ws
+    check(L.inch_mp_gemm(M, N, K, _ptr(A), A.stride(0), A.stride(1), _ptr(B), B.stride(0), B.stride(1), _ptr(C),
+                         C.stride(0), float(beta), _ptr(ws), ws.numel(), _stream()))
+    _count(1 if need <= 256 else 2)
+    return C
+
+
 def mp(name, *args):
     """Call inch_mp_<name>(*args, stream): tensors become device pointers."""
     conv = [(_ptr(a) if isinstance(a, torch.Tensor) else a) for a in args]

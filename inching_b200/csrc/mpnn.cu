@@ -144,6 +144,99 @@ __global__ void k_adam(float* __restrict__ w, const float* __restrict__ g, float
   }
 }
 
+// Dense layers: C = A B (+ beta C) in FP32 with arbitrary element strides, so the
+// same kernel serves X W, X^T dY (weight gradients, a reduction over the long
+// dimension) and dY W^T.  64 x 64 output tiles, K in chunks of 16 staged in shared
+// memory, 4 x 4 outputs per thread.  Small output grids over a long K split K over
+// gridDim.z into per-split partial tiles, added in a fixed order by k_gemm_reduce
+// (deterministic).
+constexpr int kGM = 64, kGN = 64, kGK = 16;
+
+__global__ void __launch_bounds__(256)
+k_gemm(int M, int N, int K, const float* __restrict__ A, int64_t sai, int64_t sak, const float* __restrict__ B,
+       int64_t sbk, int64_t sbn, float* C, int64_t ldc, float beta, int kchunk, float* __restrict__ part) {
+  __shared__ float As[kGK][kGM + 4];
+  __shared__ float Bs[kGK][kGN + 4];
+  const int bm = blockIdx.y * kGM, bn = blockIdx.x * kGN;
+  const int k_beg = blockIdx.z * kchunk;
+  const int k_end = (K - k_beg) < kchunk ? K : k_beg + kchunk;
+  const int tx = threadIdx.x & 15, ty = threadIdx.x >> 4;
+  float acc[4][4];
+#pragma unroll
+  for (int r = 0; r < 4; ++r)
+#pragma unroll
+    for (int c = 0; c < 4; ++c) acc[r][c] = 0.f;
+  for (int k0 = k_beg; k0 < k_end; k0 += kGK) {
+    // stage the A and B tiles, consecutive threads along whichever index is unit-stride
+    for (int t = threadIdx.x; t < kGM * kGK; t += 256) {
+      const int mm = (sak == 1) ? t / kGK : t % kGM;
+      const int kk = (sak == 1) ? t % kGK : t / kGM;
+      const int gi = bm + mm, gk = k0 + kk;
+      As[kk][mm] = (gi < M && gk < k_end) ? A[(int64_t)gi * sai + (int64_t)gk * sak] : 0.f;
+    }
+    for (int t = threadIdx.x; t < kGN * kGK; t += 256) {
+      const int nn = (sbn == 1) ? t % kGN : t / kGK;
+      const int kk = (sbn == 1) ? t / kGN : t % kGK;
+      const int gj = bn + nn, gk = k0 + kk;
+      Bs[kk][nn] = (gj < N && gk < k_end) ? B[(int64_t)gk * sbk + (int64_t)gj * sbn] : 0.f;
+    }
+    __syncthreads();
+#pragma unroll
+    for (int kk = 0; kk < kGK; ++kk) {
+      float a[4], b[4];
+#pragma unroll
+      for (int r = 0; r < 4; ++r) a[r] = As[kk][ty * 4 + r];
+#pragma unroll
+      for (int c = 0; c < 4; ++c) b[c] = Bs[kk][tx * 4 + c];
+#pragma unroll
+      for (int r = 0; r < 4; ++r)
+#pragma unroll
+        for (int c = 0; c < 4; ++c) acc[r][c] = fmaf(a[r], b[c], acc[r][c]);
+    }
+    __syncthreads();
+  }
+#pragma unroll
+  for (int r = 0; r < 4; ++r) {
+    const int i = bm + ty * 4 + r;
+    if (i >= M) continue;
+#pragma unroll
+    for (int c = 0; c < 4; ++c) {
+      const int j = bn + tx * 4 + c;
+      if (j >= N) continue;
+      if (part != nullptr) {
+        part[((int64_t)blockIdx.z * M + i) * N + j] = acc[r][c];
+      } else {
+        float* cp = C + (int64_t)i * ldc + j;
+        *cp = beta != 0.f ? fmaf(beta, *cp, acc[r][c]) : acc[r][c];
+      }
+    }
+  }
+}
+
+__global__ void k_gemm_reduce(int M, int N, int splits, const float* __restrict__ part, float* C, int64_t ldc,
+                              float beta) {
+  const int64_t total = (int64_t)M * N;
+  for (int64_t t = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; t < total; t += (int64_t)gridDim.x * blockDim.x) {
+    const int64_t i = t / N, j = t % N;
+    float sum = 0.f;
+    for (int sp = 0; sp < splits; ++sp) sum += part[sp * total + t];
+    float* cp = C + i * ldc + j;
+    *cp = beta != 0.f ? fmaf(beta, *cp, sum) : sum;
+  }
+}
+
+// K splits of a (M x N) product over K: enough blocks for the 148 SMs when the
+// output grid alone is small and K is long.
+int gemm_splits(int M, int N, int K) {
+  const int tiles = ((M + kGM - 1) / kGM) * ((N + kGN - 1) / kGN);
+  if (tiles >= 148 || K <= 2048) return 1;
+  int sp = (2 * 148 + tiles - 1) / tiles;
+  const int by_k = (K + 1023) / 1024;
+  if (sp > by_k) sp = by_k;
+  if (sp > 64) sp = 64;
+  return sp < 1 ? 1 : sp;
+}
+
 int blocks(int64_t work) { return grid_for(work, kT, 148 * 16); }
 
 }  // namespace
@@ -218,4 +311,33 @@ extern "C" inch_status inch_mp_adam(float* w, const float* g, float* m1, float* 
   const float c1 = 1.f - powf(b1, (float)step), c2 = 1.f - powf(b2, (float)step);
   k_adam<<<blocks(n), kT, 0, s>>>(w, g, m1, m2, n, lr, b1, b2, eps, c1, c2);
   MP_CHECK();
+}
+
+extern "C" size_t inch_mp_gemm_workspace_size(int32_t M, int32_t N, int32_t K) {
+  const int sp = gemm_splits(M, N, K);
+  return sp > 1 ? (size_t)sp * M * N * sizeof(float) + 256 : 256;
+}
+
+extern "C" inch_status inch_mp_gemm(int32_t M, int32_t N, int32_t K, const float* A, int64_t sai, int64_t sak,
+                                    const float* B, int64_t sbk, int64_t sbn, float* C, int64_t ldc, float beta,
+                                    void* ws, size_t ws_bytes, cudaStream_t s) {
+  INCH_REQUIRE(A && B && C && M >= 1 && N >= 1 && K >= 1 && ldc >= N, INCH_INVALID_ARG, "inch_mp_gemm: bad args");
+  const int sp = gemm_splits(M, N, K);
+  float* part = nullptr;
+  int kchunk = K;
+  if (sp > 1) {
+    INCH_REQUIRE(ws != nullptr && ws_bytes >= inch_mp_gemm_workspace_size(M, N, K), INCH_OOM,
+                 "inch_mp_gemm: workspace of %zu bytes, need %zu", ws_bytes, inch_mp_gemm_workspace_size(M, N, K));
+    part = static_cast<float*>(ws);
+    kchunk = ((K + sp - 1) / sp + kGK - 1) / kGK * kGK;
+  }
+  const int zs = (K + kchunk - 1) / kchunk;
+  dim3 g((N + kGN - 1) / kGN, (M + kGM - 1) / kGM, zs);
+  k_gemm<<<g, 256, 0, s>>>(M, N, K, A, sai, sak, B, sbk, sbn, C, ldc, beta, kchunk, part);
+  INCH_LAUNCH_CHECK();
+  if (part != nullptr) {
+    k_gemm_reduce<<<blocks((int64_t)M * N), kT, 0, s>>>(M, N, zs, part, C, ldc, beta);
+    INCH_LAUNCH_CHECK();
+  }
+  return INCH_OK;
 }

@@ -804,6 +804,37 @@ extern "C" inch_status inch_spmm_seg(int32_t prec, int64_t n_atoms, const int64_
   return INCH_OK;
 }
 
+extern "C" inch_status inch_spmm_seg_ws(int32_t prec, int64_t n_atoms, const int64_t* rowptr, const void* ent,
+                                        const void* diag, const void* X, int64_t ldx, int32_t b, void* Y,
+                                        int64_t ldy, const void* Yin, int64_t ldyin, const int32_t* atom_seg,
+                                        const double* seg_coef, void* ws, size_t ws_bytes, cudaStream_t stream) {
+  INCH_REQUIRE(prec == 32 || prec == 64, INCH_INVALID_ARG, "inch_spmm_seg_ws: prec must be 32 or 64");
+  INCH_REQUIRE(rowptr && ent && diag && X && Y && atom_seg && seg_coef && ws, INCH_INVALID_ARG,
+               "inch_spmm_seg_ws: NULL argument");
+  INCH_REQUIRE(n_atoms >= 1 && n_atoms < (int64_t(1) << 31), INCH_INVALID_ARG,
+               "inch_spmm_seg_ws: n_atoms out of range");
+  INCH_REQUIRE(b >= 1 && b <= (prec == 32 ? 128 : 64) && ldx >= b && ldy >= b && X != Y, INCH_INVALID_ARG,
+               "inch_spmm_seg_ws: bad b / leading dimension / aliasing");
+  INCH_REQUIRE(Yin == nullptr || ldyin >= b, INCH_INVALID_ARG, "inch_spmm_seg_ws: ldyin below b");
+  INCH_REQUIRE(((uintptr_t)ent & 15) == 0 && ((uintptr_t)diag & 15) == 0, INCH_INVALID_ARG,
+               "inch_spmm_seg_ws: store buffers must be 16-byte aligned");
+  Carver c(ws, ws_bytes);
+  int* counter = c.take<int>(1);
+  INCH_REQUIRE(c.ok, INCH_OOM, "inch_spmm_seg_ws: workspace too small");
+  Epi ep{0.0, 0.0, 0.0, 0.0, 0, 0, Yin != nullptr ? 1 : 0};
+  ep.seg_coef = seg_coef;
+  ep.atom_seg = atom_seg;
+  cudaError_t err;
+  if (prec == 32)
+    err = run<float>(n_atoms, rowptr, ent, diag, X, ldx, b, Y, ldy, Yin, ldyin, nullptr, 0, ep, nullptr, 0.0,
+                     nullptr, nullptr, stream, counter);
+  else
+    err = run<double>(n_atoms, rowptr, ent, diag, X, ldx, b, Y, ldy, Yin, ldyin, nullptr, 0, ep, nullptr, 0.0,
+                      nullptr, nullptr, stream, counter);
+  INCH_REQUIRE(err == cudaSuccess, INCH_CUDA_ERROR, "inch_spmm_seg_ws: %s", cudaGetErrorString(err));
+  return INCH_OK;
+}
+
 // ---------------------------------------------------------------------------
 // Chebyshev filters as single library calls (the SpMM above, looped inside the
 // library with its fused epilogue; the caller provides every buffer).

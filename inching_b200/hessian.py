@@ -241,8 +241,9 @@ class HessianStore:
             pw = t["pw64"] if prec == 64 else t["pw32"]
             return _native.spmm_tiles_seg(prec, self.n_atoms, t["uptr"], t["pptr"], t["urec"], pw, diag, X, out,
                                           atom_seg, seg_coef, Yin=Yin)
-        for c0 in range(0, X.shape[1], 64):
-            sl = slice(c0, min(c0 + 64, X.shape[1]))
+        panel = 128 if prec == 32 else 64
+        for c0 in range(0, X.shape[1], panel):
+            sl = slice(c0, min(c0 + panel, X.shape[1]))
             _native.spmm_seg(prec, self.n_atoms, self.rowptr, ent, diag, X[:, sl], out[:, sl], atom_seg, seg_coef,
                              Yin=None if Yin is None else Yin[:, sl])
         return out

@@ -120,6 +120,27 @@ def _param_shapes():
     return shapes
 
 
+def _mm(A, B, out=None, accumulate=False):
+    """A @ B (+ out) on the package's dense-layer kernel (FP32); A and B may be
+    transposed views."""
+    if out is None:
+        out = torch.empty((A.shape[0], B.shape[1]), dtype=torch.float32, device=A.device)
+    return _native.mp_gemm(A, B, out, 1.0 if accumulate else 0.0)
+
+
+_ones = {}
+
+
+def _colsum(Y, out):
+    """out (1, F) += column sums of Y (rows, F), as ones^T Y on the same kernel."""
+    r = Y.shape[0]
+    o = _ones.get((Y.device, r))
+    if o is None:
+        o = torch.ones((1, r), dtype=torch.float32, device=Y.device)
+        _ones[(Y.device, r)] = o
+    return _native.mp_gemm(o, Y, out, 1.0)
+
+
 class WarmStartMPNN:
     def __init__(self, device="cuda", seed=0):
         self.shapes = _param_shapes()
@@ -165,26 +186,26 @@ class WarmStartMPNN:
     def forward(self, G: BeadGraph):
         p = self.p
         c = {}
-        h = G.x @ p["W0"]
+        h = _mm(G.x, p["W0"])
         _native.mp("bias_relu", h, p["b0"], G.n, WIDTH)
         c["h0"] = h
         hs = [h]
         for l in range(LAYERS):
             Z = torch.empty((G.E, WIDTH + EDGE_F), dtype=torch.float32, device=h.device)
             _native.mp("edge_concat", h, G.ef, G.src, G.E, WIDTH, EDGE_F, Z)
-            A = Z @ p[f"Wm{l}"]
+            A = _mm(Z, p[f"Wm{l}"])
             _native.mp("bias_relu", A, p[f"bm{l}"], G.E, WIDTH)
             M = torch.empty((G.n, WIDTH), dtype=torch.float32, device=h.device)
             _native.mp("segment_sum", A, G.mp_rowptr, G.n, WIDTH, M)
             U = torch.cat([h, M], dim=1)
-            T = U @ p[f"Wu{l}"]
+            T = _mm(U, p[f"Wu{l}"])
             _native.mp("bias_relu", T, p[f"bu{l}"], G.n, WIDTH)
             c[l] = (Z, A, U, T)
             h = h + T
             hs.append(h)
         R = torch.empty((G.E, WIDTH + EDGE_F), dtype=torch.float32, device=h.device)
         _native.mp("edge_pair", h, G.ef, G.src, G.dst, G.E, WIDTH, EDGE_F, R)
-        s = (R @ p["wo"]).reshape(-1) + p["bo"]
+        s = _mm(R, p["wo"]).reshape(-1) + p["bo"]
         s = s.contiguous()
         gamma = torch.empty(G.E, dtype=torch.float64, device=h.device)
         _native.mp("softplus", s, G.E, GAMMA_FLOOR, gamma, None, None)
@@ -196,8 +217,8 @@ class WarmStartMPNN:
         p, g = self.p, self.g
         ds = torch.empty(G.E, dtype=torch.float32, device=dgamma.device)
         _native.mp("softplus", c["s"], G.E, GAMMA_FLOOR, None, dgamma.contiguous(), ds)
-        g["wo"] += c["R"].t() @ ds[:, None]
-        g["bo"] += ds.sum().reshape(1)
+        _mm(c["R"].t(), ds[:, None], out=g["wo"], accumulate=True)
+        _colsum(ds[:, None], g["bo"][None, :])
         dR = (ds[:, None] * p["wo"].reshape(1, -1)).contiguous()
         dh = torch.zeros((G.n, WIDTH), dtype=torch.float32, device=ds.device)
         _native.mp("edge_pair_bwd", dR, G.src, G.dst, G.E, WIDTH, EDGE_F, dh)
@@ -205,22 +226,22 @@ class WarmStartMPNN:
             Z, A, U, T = c[l]
             dT = dh.clone()
             _native.mp("relu_bwd", dT, T, dT.numel())
-            g[f"Wu{l}"] += U.t() @ dT
-            g[f"bu{l}"] += dT.sum(dim=0)
-            dU = dT @ p[f"Wu{l}"].t()
+            _mm(U.t(), dT, out=g[f"Wu{l}"], accumulate=True)
+            _colsum(dT, g[f"bu{l}"][None, :])
+            dU = _mm(dT, p[f"Wu{l}"].t())
             dM = dU[:, WIDTH:].contiguous()
             dh = dh + dU[:, :WIDTH]
             dA = torch.empty((G.E, WIDTH), dtype=torch.float32, device=ds.device)
             _native.mp("segment_sum_bwd", dM, G.mp_rowptr, G.dst, G.E, WIDTH, dA)
             _native.mp("relu_bwd", dA, A, dA.numel())
-            g[f"Wm{l}"] += Z.t() @ dA
-            g[f"bm{l}"] += dA.sum(dim=0)
-            dZ = (dA @ p[f"Wm{l}"].t()).contiguous()
+            _mm(Z.t(), dA, out=g[f"Wm{l}"], accumulate=True)
+            _colsum(dA, g[f"bm{l}"][None, :])
+            dZ = _mm(dA, p[f"Wm{l}"].t())
             dh = dh.contiguous()
             _native.mp("edge_concat_bwd", dZ, G.src, G.E, WIDTH, EDGE_F, dh)
         _native.mp("relu_bwd", dh, c["h0"], dh.numel())
-        g["W0"] += G.x.t() @ dh
-        g["b0"] += dh.sum(dim=0)
+        _mm(G.x.t(), dh, out=g["W0"], accumulate=True)
+        _colsum(dh, g["b0"][None, :])
 
     def adam(self, lr=1e-3, b1=0.9, b2=0.999, eps=1e-8):
         self.step += 1

@@ -195,6 +195,7 @@ inch_status inch_hessian_assemble_pbc_xy(const double* X_dev, int64_t n_atoms, d
  *   hf_grad          out[e] = 1/2 sum_t c[t] (u_e . (V_t[a] - V_t[b]))^2
  *                    (Hellmann-Feynman eigenvalue gradient of the bead Hessian)
  *   adam             one bias-corrected Adam step
+ *   gemm             the dense layers (forward, weight and input gradients)
  * ------------------------------------------------------------------------- */
 inch_status inch_mp_edge_concat(const float* H, const float* EF, const int32_t* src, int64_t E, int32_t F,
                                 int32_t G, float* Z, cudaStream_t stream);
@@ -217,6 +218,15 @@ inch_status inch_mp_hf_grad(const double* P, const int64_t* rowptr, const int32_
                             cudaStream_t stream);
 inch_status inch_mp_adam(float* w, const float* g, float* m1, float* m2, int64_t n, float lr, float b1, float b2,
                          float eps, int32_t step, cudaStream_t stream);
+/* The network's dense layers: C = A B + beta C in FP32, with element (i, k) of A at
+ * A[i*sai + k*sak] and (k, j) of B at B[k*sbk + j*sbn] (so transposed operands are
+ * strides), C row-major with leading dimension ldc.  A product with a small output
+ * and a long K splits K into partial tiles added in a fixed order (deterministic);
+ * ws: inch_mp_gemm_workspace_size(M, N, K) bytes.  No reference counterpart. */
+size_t inch_mp_gemm_workspace_size(int32_t M, int32_t N, int32_t K);
+inch_status inch_mp_gemm(int32_t M, int32_t N, int32_t K, const float* A, int64_t sai, int64_t sak,
+                         const float* B, int64_t sbk, int64_t sbn, float* C, int64_t ldc, float beta,
+                         void* ws_dev, size_t ws_bytes, cudaStream_t stream);
 
 /* ---------------------------------------------------------------------------
  * Hessian x multivector with fused epilogue.  X and Y are (3N, b) row-major with
@@ -257,6 +267,14 @@ inch_status inch_spmm_seg(int32_t prec, int64_t n_atoms, const int64_t* rowptr_d
                           const void* X_dev, int64_t ldx, int32_t b,
                           void* Y_dev, int64_t ldy, const void* Yin_dev, int64_t ldyin,
                           const int32_t* atom_seg_dev, const double* seg_coef_dev, cudaStream_t stream);
+/* inch_spmm_seg with a workspace (inch_spmm_workspace_size bytes): the wide-block
+ * kernel then hands out its rows from the counter in it (inch_spmm_traversal) and
+ * FP32 takes up to 128 columns per call, as in inch_spmm.  Used by the CUDA-graph
+ * Chebyshev filter.  Calls sharing a workspace must not overlap on the GPU. */
+inch_status inch_spmm_seg_ws(int32_t prec, int64_t n_atoms, const int64_t* rowptr_dev, const void* ent_dev,
+                             const void* diag_dev, const void* X_dev, int64_t ldx, int32_t b, void* Y_dev,
+                             int64_t ldy, const void* Yin_dev, int64_t ldyin, const int32_t* atom_seg_dev,
+                             const double* seg_coef_dev, void* ws_dev, size_t ws_bytes, cudaStream_t stream);
 
 /* Launch shape of the wide-block (b >= 8) SpMM kernel for this process: threads
  * per block (256, 512 or 1024) and resident blocks per SM (1..8); each block walks

@@ -153,3 +153,33 @@ def test_pipeline_with_shipped_weights():
     assert i1["max_rel_residual"] <= 1.5e-6
     assert i1["iterations"] <= i0["iterations"]
     assert float(((e1 - e0).abs() / e0).max()) < 1e-6
+
+
+@pytest.mark.parametrize("M,N,K,ta,tb", [(300, 128, 137, False, False), (7800, 128, 263, False, False),
+                                         (263, 128, 60000, True, False), (1, 128, 50000, False, False),
+                                         (5000, 263, 128, False, True), (129, 1, 263, False, False)])
+def test_dense_layer_kernel_matches_torch(M, N, K, ta, tb):
+    """The network's dense-layer kernel (inch_mp_gemm) against a torch FP32 matmul of
+    the same operands: forward (X W), weight gradient (X^T dY, long K with the
+    deterministic split-K), input gradient (dY W^T), column sums, a single column;
+    accumulating into C with beta = 1.  Tolerance 1e-5 of the largest output."""
+    from inching_b200 import _native
+    g = torch.Generator(device="cuda")
+    g.manual_seed(M + N + K)
+    A = torch.randn((K, M) if ta else (M, K), generator=g, device="cuda")
+    B = torch.randn((N, K) if tb else (K, N), generator=g, device="cuda")
+    Av = A.t() if ta else A
+    Bv = B.t() if tb else B
+    ref = Av @ Bv
+    C = torch.empty((M, N), device="cuda")
+    _native.mp_gemm(Av, Bv, C)
+    scale = float(ref.abs().max())
+    assert float((C - ref).abs().max()) <= 1e-5 * scale * max(1.0, K ** 0.5 / 10)
+    C0 = torch.randn((M, N), generator=g, device="cuda")
+    C1 = C0.clone()
+    _native.mp_gemm(Av, Bv, C1, beta=1.0)
+    assert float((C1 - (C0 + ref)).abs().max()) <= 1e-5 * (scale + float(C0.abs().max())) * max(1.0, K ** 0.5 / 10)
+    # deterministic: the same call twice gives the same bits
+    C2 = torch.empty((M, N), device="cuda")
+    _native.mp_gemm(Av, Bv, C2)
+    assert torch.equal(C, C2)
