@@ -174,3 +174,33 @@ def test_store_matches_reference_dense_hessian(name):
     E[torch.from_numpy(cols).cuda(), torch.arange(len(cols), device="cuda")] = 1.0
     Y = H.matmul(E).cpu().numpy()
     assert np.abs(Y[:, :len(cols)] - Href[:, cols]).max() <= TOL64 * scale
+
+
+@pytest.mark.parametrize("n", [1, 2, 5, 9, 33])
+@pytest.mark.parametrize("prec", [64, 32])
+def test_tiny_stores_every_width_and_traversal(n, prec):
+    """Stores smaller than one row chunk, with an isolated atom and a coincident
+    pair: every tile width (1 .. 130 columns) and every row traversal of the wide
+    kernel gives the oracle's product."""
+    from inching_b200 import _native
+    from inching_b200.hessian import HessianStore
+    rng = np.random.default_rng(n)
+    X = rng.random((n, 3)) * 1.2
+    if n >= 5:
+        X[-1] = X[-1] + 5.0          # isolated atom
+        X[1] = X[0]                  # coincident pair (d = 0: no spring)
+    A, Ad = oh.hessian_lower(X, 8.0, 1.0)
+    H = HessianStore(X, 8.0, plus_i=1.0)
+    scale = max(float(abs(oh.full_from_lower(A, Ad)).max()), 1.0)
+    dt = torch.float64 if prec == 64 else torch.float32
+    try:
+        for trav in (0, 1, 2):
+            _native.spmm_tune(256, 5, trav)
+            for b in (1, 3, 8, 64, 128, 130):
+                Xv = rng.standard_normal((3 * n, b))
+                ref = np.stack([oh.krylov_av(A, Ad, Xv[:, c]) for c in range(b)], axis=1)
+                Y = H.matmul(torch.from_numpy(Xv).to("cuda", dt).contiguous(), prec=prec)
+                tol = (TOL64 if prec == 64 else TOL32) * scale * np.abs(Xv).max() * 10
+                assert np.abs(Y.double().cpu().numpy() - ref).max() <= tol, (trav, b)
+    finally:
+        _native.spmm_tune(256, 5, 1)
