@@ -72,7 +72,8 @@ def parse():
     ap.add_argument("--degree", type=int, default=None, help="cube2400k: Chebyshev filter degree (default: the "
                     "solver's size rule)")
     ap.add_argument("--profile", action="store_true", help="cube2400k: CUDA-event phase times of the solver")
-    ap.add_argument("--layout", default="tiles", choices=["tiles", "pairs"], help="store layout for --kernel-only")
+    ap.add_argument("--layout", default="groups", choices=["groups", "pairs", "tiles"],
+                    help="store layout for --kernel-only (groups: the row-group layout the solvers use for FP32)")
     ap.add_argument("--traversal", type=int, default=None, choices=[0, 1, 2],
                     help="row traversal of the wide pair kernel (--kernel-only)")
     ap.add_argument("--band-panel", type=int, default=None, choices=[64, 128],
@@ -97,7 +98,7 @@ def run_kernel_only(args):
     order, _ = graph.cuthill_mckee(Xd, 8.0)
     prec = 32 if args.kernel_only == "spmm32" else 64
     H = HessianStore(Xd[order], 8.0, 1.0, precisions=("f32",) if prec == 32 else ("f64",),
-                     tiles=args.layout == "tiles")
+                     tiles=args.layout == "tiles", groups=2 if args.layout == "groups" else 0)
     dt = torch.float32 if prec == 32 else torch.float64
     g = torch.Generator(device="cuda")
     g.manual_seed(0)

@@ -115,6 +115,17 @@ _SIGS = {
     "inch_spmm_tiles_seg": (ctypes.c_int, [c_int32, c_int64, c_void_p, c_void_p, c_void_p, c_void_p, c_void_p,
                                            c_void_p, c_int64, c_int32, c_void_p, c_int64, c_void_p, c_int64,
                                            c_void_p, c_void_p, c_void_p]),
+    "inch_group_store_workspace_size": (c_size_t, [c_int64, c_int32]),
+    "inch_group_store_count": (ctypes.c_int, [c_void_p, c_void_p, c_int64, c_int32, c_void_p, POINTER(c_int64),
+                                              c_void_p, c_size_t, c_void_p]),
+    "inch_group_store_fill": (ctypes.c_int, [c_void_p, c_void_p, c_int64, c_int32, c_void_p, c_void_p, c_void_p]),
+    "inch_spmm_group_tune": (ctypes.c_int, [c_int32]),
+    "inch_spmm_groups": (ctypes.c_int, [c_int64, c_int32, c_void_p, c_void_p, c_void_p, c_void_p, c_int64, c_int32,
+                                        c_void_p, c_int64, c_void_p, c_int64, c_void_p, c_int64, c_void_p,
+                                        POINTER(SpmmEpilogue), c_void_p, c_size_t, c_void_p]),
+    "inch_spmm_groups_seg": (ctypes.c_int, [c_int64, c_int32, c_void_p, c_void_p, c_void_p, c_void_p, c_int64,
+                                            c_int32, c_void_p, c_int64, c_void_p, c_int64, c_void_p, c_void_p,
+                                            c_void_p, c_size_t, c_void_p]),
     "inch_spmm_band_tune": (ctypes.c_int, [c_int32]),
     "inch_spmm_band_status": (ctypes.c_int, [POINTER(c_int32)]),
     "inch_hessian_assemble_weighted": (ctypes.c_int, [c_void_p, c_int64, c_double, c_double, c_void_p, c_void_p,
@@ -477,6 +488,107 @@ def spmm_tiles_seg(prec, n_atoms, uptr, pptr, urec, pw, diag, X, Y, atom_seg, se
     check(L.inch_spmm_tiles_seg(prec, n_atoms, _ptr(uptr), _ptr(pptr), _ptr(urec), _ptr(pw), _ptr(diag), _ptr(X),
                                 ldx, b, _ptr(Y), ldy, _ptr(Yin), ldyin, _ptr(atom_seg), _ptr(seg_coef), _stream()))
     _count(band_panels(prec, b))
+    return Y
+
+
+# ---------------------------------------------------------------------------
+# Row-group store (FP32; R consecutive rows merged over their neighbour lists)
+# ---------------------------------------------------------------------------
+def group_store(rowptr, ent32, n_atoms, rows_per_group=2):
+    """(group_ptr int64 (G+1,), group_ent float32 (U*R, 4), n_union) built from the
+    FP32 pair entries: R = 2 or 4 consecutive rows per group, each group's unions
+    padded to a multiple of 16."""
+    L = lib()
+    _require_cuda(ent32, "ent32", torch.float32)
+    R = int(rows_per_group)
+    if R not in (2, 4):
+        raise AssertionError("ABORTED. rows_per_group must be 2 or 4")
+    dev = ent32.device
+    ng = (n_atoms + R - 1) // R
+    gptr = torch.empty(ng + 1, dtype=torch.int64, device=dev)
+    ws = _ws(L.inch_group_store_workspace_size(n_atoms, R), dev)
+    nu = c_int64(0)
+    check(L.inch_group_store_count(_ptr(rowptr), _ptr(ent32), n_atoms, R, _ptr(gptr), ctypes.byref(nu), _ptr(ws),
+                                   ws.numel(), _stream()))
+    gent = torch.empty((max(nu.value, 1) * R, 4), dtype=torch.float32, device=dev)
+    check(L.inch_group_store_fill(_ptr(rowptr), _ptr(ent32), n_atoms, R, _ptr(gptr), _ptr(gent), _stream()))
+    _count(4)
+    return gptr, gent, nu.value
+
+
+def group_tiles(b, aligned4=True, aligned2=True):
+    """Kernel tiles of one row-group product of b columns (128 / 64 / 32, the last
+    one partial)."""
+    n, c0 = 0, 0
+    while c0 < b:
+        rem = b - c0
+        if rem >= 128 and aligned4:
+            c0 += 128
+        elif rem >= 64 and aligned2:
+            c0 += 64
+        else:
+            c0 += min(rem, 32)
+        n += 1
+    return n
+
+
+def _aligned(m, k):
+    if m is None:
+        return True
+    ld = 1 if m.dim() == 1 else m.stride(0)
+    return ld % k == 0 and m.data_ptr() % (4 * k) == 0
+
+
+def spmm_group_tune(unroll=0):
+    """Unions in flight per warp of the row-group product (0: the default, 16 on
+    128-column tiles and 8 on narrower ones; or 2, 4, 8, 16) for this process
+    (autotuner hook)."""
+    check(lib().inch_spmm_group_tune(int(unroll)))
+
+
+def spmm_groups(n_atoms, rows_per_group, gptr, gent, diag, X, Y, *, alpha=1.0, gamma=0.0, beta=0.0, Yin=None,
+                acc=None, mu=0.0, Q=None, hot_shift=0.0):
+    """Same contract as spmm() in FP32, on the row-group store (any number of columns)."""
+    L = lib()
+    b = 1 if X.dim() == 1 else X.shape[1]
+    ldx = 1 if X.dim() == 1 else X.stride(0)
+    ldy = 1 if Y.dim() == 1 else Y.stride(0)
+    ldyin = 0 if Yin is None else (1 if Yin.dim() == 1 else Yin.stride(0))
+    ldacc = 0 if acc is None else (1 if acc.dim() == 1 else acc.stride(0))
+    r = 0 if Q is None else Q.shape[0]
+    ep = SpmmEpilogue(alpha, gamma, beta, mu, hot_shift, r, 1 if acc is not None else 0)
+    dev = X.device
+    key = (dev.index, r > 0)
+    ws = _ws_cache.get(key)
+    if ws is None:
+        ws = _ws(L.inch_spmm_workspace_size(n_atoms, b, r), dev)
+        _ws_cache[key] = ws
+    check(L.inch_spmm_groups(n_atoms, rows_per_group, _ptr(gptr), _ptr(gent), _ptr(diag), _ptr(X), ldx, b, _ptr(Y),
+                             ldy, _ptr(Yin), ldyin, _ptr(acc), ldacc, _ptr(Q), ctypes.byref(ep), _ptr(ws),
+                             ws.numel(), _stream()))
+    blocks = [X, Y] + ([Yin] if beta != 0.0 else []) + ([acc] if acc is not None else [])
+    nt = group_tiles(b, all(_aligned(m, 4) for m in blocks), all(_aligned(m, 2) for m in blocks))
+    _count(nt * (3 if r > 0 else 1))
+    return Y
+
+
+def spmm_groups_seg(n_atoms, rows_per_group, gptr, gent, diag, X, Y, atom_seg, seg_coef, Yin=None):
+    """spmm_seg() on the row-group store (FP32, any number of columns)."""
+    L = lib()
+    b = 1 if X.dim() == 1 else X.shape[1]
+    ldx = 1 if X.dim() == 1 else X.stride(0)
+    ldy = 1 if Y.dim() == 1 else Y.stride(0)
+    ldyin = 0 if Yin is None else (1 if Yin.dim() == 1 else Yin.stride(0))
+    dev = X.device
+    ws = _ws_cache.get((dev.index, False))
+    if ws is None:
+        ws = _ws(L.inch_spmm_workspace_size(n_atoms, b, 0), dev)
+        _ws_cache[(dev.index, False)] = ws
+    check(L.inch_spmm_groups_seg(n_atoms, rows_per_group, _ptr(gptr), _ptr(gent), _ptr(diag), _ptr(X), ldx, b,
+                                 _ptr(Y), ldy, _ptr(Yin), ldyin, _ptr(atom_seg), _ptr(seg_coef), _ptr(ws),
+                                 ws.numel(), _stream()))
+    blocks = [X, Y] + ([Yin] if Yin is not None else [])
+    _count(group_tiles(b, all(_aligned(m, 4) for m in blocks), all(_aligned(m, 2) for m in blocks)))
     return Y
 
 

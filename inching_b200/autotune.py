@@ -4,8 +4,10 @@ For a given store, block width and precision it times the candidate launch
 configurations of the SpMM with CUDA events on the current stream and keeps the
 fastest, for the process and on the store itself (the store re-applies its own
 choice before each product, so stores of different sizes keep their own):
-  * layout: the pair layout (one entry per neighbour pair) or the band-tile layout
-    (8-row tiles with merged neighbour unions), when the store has tiles;
+  * layout: the pair layout (one entry per neighbour pair), the row-group layout
+    (FP32; 2 consecutive rows merged over their neighbour lists, one gather of X_j
+    for both), when the store has it, or the band-tile layout (8-row tiles with
+    merged neighbour unions), when the store has tiles;
   * lane-group kernel block shape: 256 x 5, 256 x 4, 512 x 2 blocks/SM;
   * row traversal of the lane-group kernel: fixed grid stride (the warps of a
     block on neighbouring rows share their X_j rows in L1), or chunks of rows
@@ -23,7 +25,7 @@ from . import _native
 
 # (layout, threads per block (0: whole-warp kernel), blocks per SM, traversal)
 CANDIDATES = (("pairs", 256, 5, 1), ("pairs", 256, 5, 0), ("pairs", 256, 5, 2), ("pairs", 256, 4, 1),
-              ("pairs", 512, 2, 1), ("pairs", 0, 4, 0), ("tiles", 256, 5, 1))
+              ("pairs", 512, 2, 1), ("pairs", 0, 4, 0), ("groups", 256, 5, 1), ("tiles", 256, 5, 1))
 _cache = {}
 
 
@@ -39,9 +41,11 @@ def _apply(H, cfg):
 def apply_config(H, cfg):
     """Make cfg = (layout, threads, blocks per SM, traversal) the current choice."""
     layout, threads, bps, trav = cfg
-    if layout == "pairs":
+    if layout in ("pairs", "groups"):
         _native.spmm_tune(threads, bps, trav)
     H.use_tiles = layout == "tiles"
+    if getattr(H, "groups", None) is not None:
+        H.use_groups = layout == "groups"
 
 
 def cuda_event_ms(fn, reps):
@@ -77,6 +81,8 @@ def tune_spmm(H, b, prec=32, reps=3, candidates=CANDIDATES, timer=cuda_event_ms)
     table = {}
     for cfg in candidates:
         if cfg[0] == "tiles" and H.tiles is None:
+            continue
+        if cfg[0] == "groups" and (getattr(H, "groups", None) is None or prec != 32 or w < 64):
             continue
         if cfg[0] == "pairs" and not H.keep_pairs:
             continue

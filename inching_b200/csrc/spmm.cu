@@ -17,6 +17,8 @@
 // so neighbouring rows share their X_j), and reduce with xor shuffles.
 #include <atomic>
 
+#include <cub/cub.cuh>
+
 #include "common.cuh"
 
 namespace inch {
@@ -213,15 +215,84 @@ __device__ __forceinline__ void vld(const T* p, T (&x)[V]) {
 // 11x the algorithmic bytes from DRAM).
 constexpr int kRowSteps = 4;
 
+template <class T>
+__device__ __forceinline__ T mad(T a, T b, T c);
+template <>
+__device__ __forceinline__ float mad<float>(float a, float b, float c) {
+  return __fmaf_rn(a, b, c);
+}
+template <>
+__device__ __forceinline__ double mad<double>(double a, double b, double c) {
+  return __fma_rn(a, b, c);
+}
+
+template <int B, int V>
+constexpr int lanes_per_row() {
+  return (B / V) < 32 ? (B / V) : 32;
+}
+template <int B, int V>
+constexpr int cols_per_lane() {
+  return B / (lanes_per_row<B, V>() * V);
+}
+
+// Output of atom row i: h = D_i X_i + acc (acc = -sum_j w_ij (w_ij . X_j), or its
+// negation when NEG) followed by the fused epilogue.  Columns at or beyond nc (a
+// partial last tile) are neither read nor written.
+template <class T, int B, int V, bool NEG>
+__device__ __forceinline__ void row_out(int64_t i, const T (&acc)[3][cols_per_lane<B, V>()][V], int nc,
+                                        const T* __restrict__ diag, const T* __restrict__ X, int64_t ldx, T* Y,
+                                        int64_t ldy, const T* Yin, int64_t ldyin, T* __restrict__ Acc,
+                                        int64_t ldacc, int c0, const Epi& ep, const double* __restrict__ Q,
+                                        int64_t ndof, const double* s_coef, int cl) {
+  constexpr int LPR = lanes_per_row<B, V>();
+  constexpr int CPL = cols_per_lane<B, V>();
+  const T* d = diag + 8 * i;
+  const T dxx = d[0], dyy = d[1], dzz = d[2], dxy = d[3], dxz = d[4], dyz = d[5];
+  const int64_t r0 = 3 * i;
+  double al = ep.alpha, ga = ep.gamma, be = ep.beta;
+  if (ep.seg_coef != nullptr) {
+    const int sg = __ldg(ep.atom_seg + i);
+    al = __ldg(ep.seg_coef + 3 * sg);
+    ga = __ldg(ep.seg_coef + 3 * sg + 1);
+    be = __ldg(ep.seg_coef + 3 * sg + 2);
+  }
+#pragma unroll
+  for (int t = 0; t < CPL; ++t) {
+#pragma unroll
+    for (int v = 0; v < V; ++v) {
+      const int c = (t * LPR + cl) * V + v;
+      if (c >= nc) continue;
+      const T x0 = X[r0 * ldx + c0 + c], x1 = X[(r0 + 1) * ldx + c0 + c], x2 = X[(r0 + 2) * ldx + c0 + c];
+      const T a0 = NEG ? -acc[0][t][v] : acc[0][t][v];
+      const T a1 = NEG ? -acc[1][t][v] : acc[1][t][v];
+      const T a2 = NEG ? -acc[2][t][v] : acc[2][t][v];
+      T h[3];
+      h[0] = mad(dxz, x2, mad(dxy, x1, mad(dxx, x0, a0)));
+      h[1] = mad(dyz, x2, mad(dyy, x1, mad(dxy, x0, a1)));
+      h[2] = mad(dzz, x2, mad(dyz, x1, mad(dxz, x0, a2)));
+      const T xs[3] = {x0, x1, x2};
+#pragma unroll
+      for (int a = 0; a < 3; ++a) {
+        const int64_t row = r0 + a;
+        double y = al * (double)h[a] + ga * (double)xs[a];
+        if (ep.has_yin) y += be * (double)Yin[row * ldyin + c0 + c];
+        for (int q = 0; q < ep.r; ++q) y += Q[q * ndof + row] * s_coef[q * B + c];
+        Y[row * ldy + c0 + c] = (T)y;
+        if (ep.accumulate) Acc[row * ldacc + c0 + c] += (T)(ep.mu * y);
+      }
+    }
+  }
+}
+
 template <class T, int B, int V, int NT>
 __device__ __forceinline__ void cols_row(int64_t i, const int64_t* __restrict__ rowptr, const void* __restrict__ ent,
                                          const T* __restrict__ diag, const T* __restrict__ X, int64_t ldx, T* Y,
                                          int64_t ldy, const T* Yin, int64_t ldyin, T* __restrict__ Acc,
                                          int64_t ldacc, int c0, const Epi& ep, const double* __restrict__ Q,
                                          int64_t ndof, const double* s_coef, int cl) {
-  constexpr int LPR = (B / V) < 32 ? (B / V) : 32;
-  constexpr int CPL = B / (LPR * V);
-    T acc[3][CPL][V];
+  constexpr int LPR = lanes_per_row<B, V>();
+  constexpr int CPL = cols_per_lane<B, V>();
+  T acc[3][CPL][V];
 #pragma unroll
   for (int t = 0; t < CPL; ++t)
 #pragma unroll
@@ -244,45 +315,16 @@ __device__ __forceinline__ void cols_row(int64_t i, const int64_t* __restrict__ 
       vld<T, V>(xj + 2 * ldx + t * LPR * V, x2);
 #pragma unroll
       for (int v = 0; v < V; ++v) {
-        const T dot = wx * x0[v] + wy * x1[v] + wz * x2[v];
-        acc[0][t][v] -= wx * dot;
-        acc[1][t][v] -= wy * dot;
-        acc[2][t][v] -= wz * dot;
+        // dot = ((wx x0) + wy x1) + wz x2, each step one rounding (the row-group
+        // kernel repeats this order, so both layouts give the same bits)
+        const T dot = mad(wz, x2[v], mad(wy, x1[v], wx * x0[v]));
+        acc[0][t][v] = mad(-wx, dot, acc[0][t][v]);
+        acc[1][t][v] = mad(-wy, dot, acc[1][t][v]);
+        acc[2][t][v] = mad(-wz, dot, acc[2][t][v]);
       }
     }
   }
-  const T* d = diag + 8 * i;
-  const T dxx = d[0], dyy = d[1], dzz = d[2], dxy = d[3], dxz = d[4], dyz = d[5];
-  const int64_t r0 = 3 * i;
-#pragma unroll
-  for (int t = 0; t < CPL; ++t) {
-#pragma unroll
-    for (int v = 0; v < V; ++v) {
-      const int c = (t * LPR + cl) * V + v;
-      const T x0 = X[r0 * ldx + c0 + c], x1 = X[(r0 + 1) * ldx + c0 + c], x2 = X[(r0 + 2) * ldx + c0 + c];
-      T h[3];
-      h[0] = acc[0][t][v] + dxx * x0 + dxy * x1 + dxz * x2;
-      h[1] = acc[1][t][v] + dxy * x0 + dyy * x1 + dyz * x2;
-      h[2] = acc[2][t][v] + dxz * x0 + dyz * x1 + dzz * x2;
-      const T xs[3] = {x0, x1, x2};
-#pragma unroll
-      for (int a = 0; a < 3; ++a) {
-        const int64_t row = r0 + a;
-        double al = ep.alpha, ga = ep.gamma, be = ep.beta;
-      if (ep.seg_coef != nullptr) {
-        const int sg = __ldg(ep.atom_seg + i);
-        al = __ldg(ep.seg_coef + 3 * sg);
-        ga = __ldg(ep.seg_coef + 3 * sg + 1);
-        be = __ldg(ep.seg_coef + 3 * sg + 2);
-      }
-      double y = al * (double)h[a] + ga * (double)xs[a];
-        if (ep.has_yin) y += be * (double)Yin[row * ldyin + c0 + c];
-        for (int q = 0; q < ep.r; ++q) y += Q[q * ndof + row] * s_coef[q * B + c];
-        Y[row * ldy + c0 + c] = (T)y;
-        if (ep.accumulate) Acc[row * ldacc + c0 + c] += (T)(ep.mu * y);
-      }
-    }
-  }
+  row_out<T, B, V, false>(i, acc, B, diag, X, ldx, Y, ldy, Yin, ldyin, Acc, ldacc, c0, ep, Q, ndof, s_coef, cl);
 }
 
 template <class T, int B, int V, int NT>
@@ -455,7 +497,7 @@ k_spmm_warp(int64_t n_atoms, const int64_t* __restrict__ rowptr, const void* __r
 template <class T, int B>
 __global__ void __launch_bounds__(kThreads)
 k_qx_partial(const double* __restrict__ Q, int64_t ndof, const T* __restrict__ X, int64_t ldx, int c0,
-             double* __restrict__ partial) {
+             double* __restrict__ partial, int nc = B) {
   const int q = blockIdx.y, r = gridDim.y;
   const double* qr = Q + q * ndof;
   const int c = threadIdx.x % B;
@@ -463,7 +505,7 @@ k_qx_partial(const double* __restrict__ Q, int64_t ndof, const T* __restrict__ X
   const int64_t total = ndof * B;
   for (int64_t p = (int64_t)blockIdx.x * kThreads + threadIdx.x; p < total; p += (int64_t)gridDim.x * kThreads) {
     const int64_t dof = p / B;
-    acc += qr[dof] * (double)X[dof * ldx + c0 + c];
+    if (c < nc) acc += qr[dof] * (double)X[dof * ldx + c0 + c];   // columns past nc: outside the tile
   }
   __shared__ double s[kThreads];
   s[threadIdx.x] = acc;
@@ -603,6 +645,346 @@ cudaError_t run(int64_t n_atoms, const int64_t* rowptr, const void* ent, const v
     else if (rem >= 2) { TILE(2, 8) }
     else { TILE(1, 8) }
 #undef TILE
+  }
+  return e;
+}
+
+// ---------------------------------------------------------------------------
+// Row-group layout (FP32): R consecutive atom rows (R = 2 or 4) merged over their
+// sorted neighbour lists.  Group g covers atoms [R g, R g + R); its union column
+// u holds R float4 slots, slot r = {wx, wy, wz, .} of row R g + r's entry for that
+// column, or zeros when the row has none; slot 0's last field holds the column
+// index.  A row's entries keep their order inside the union (the merge is stable
+// per row and repeated columns stay separate unions), so each row sums the same
+// terms in the same order as in the pair layout, with exact zeros in between.
+// One gather of X_j then serves every row of the group that needs it: after
+// Cuthill-McKee, consecutive rows share most of their neighbours (100k-atom
+// assembly: 1.36 pairs per union for R = 2, 1.87 for R = 4), and the pair
+// product is bound by these gathers (L2 -> SM).
+// ---------------------------------------------------------------------------
+constexpr int kGroupBuildThreads = 256;
+constexpr int kGroupSteps = 4;   // groups a warp takes per grab of the counter
+// Each group's union count is padded to a multiple of kGroupPad with zero-weight
+// unions (column = the group's first atom), so the product walks whole chunks.
+constexpr int kGroupPad = 16;
+
+// One thread per group: an R-way merge over the rows' entries.  Pass 0 counts the
+// (padded) unions of each group, pass 1 writes them at gptr[g].
+template <int PASS, int R>
+__global__ void __launch_bounds__(kGroupBuildThreads)
+k_group_merge(int64_t n, const int64_t* __restrict__ rowptr, const float4* __restrict__ ent,
+              int64_t* __restrict__ count, const int64_t* __restrict__ gptr, float4* __restrict__ gent) {
+  const int64_t ng = (n + R - 1) / R;
+  for (int64_t g = (int64_t)blockIdx.x * kGroupBuildThreads + threadIdx.x; g < ng;
+       g += (int64_t)gridDim.x * kGroupBuildThreads) {
+    int64_t e[R], e1[R];
+#pragma unroll
+    for (int r = 0; r < R; ++r) {
+      const int64_t i = R * g + r;
+      e[r] = i < n ? rowptr[i] : 0;
+      e1[r] = i < n ? rowptr[i + 1] : 0;
+    }
+    const int64_t ubase = PASS == 1 ? gptr[g] : 0;
+    int64_t u = ubase;
+    for (;;) {
+      int head[R];
+      int m = 0x7fffffff;
+#pragma unroll
+      for (int r = 0; r < R; ++r) {
+        head[r] = e[r] < e1[r] ? __float_as_int(ent[e[r]].w) : 0x7fffffff;
+        m = min(m, head[r]);
+      }
+      if (m == 0x7fffffff) break;
+#pragma unroll
+      for (int r = 0; r < R; ++r) {
+        const bool take = head[r] == m;
+        if (PASS == 1) {
+          float4 w = take ? ent[e[r]] : make_float4(0.f, 0.f, 0.f, 0.f);
+          w.w = r == 0 ? __int_as_float(m) : 0.f;
+          gent[R * u + r] = w;
+        }
+        if (take) ++e[r];
+      }
+      ++u;
+    }
+    const int64_t u_end = ubase + (u - ubase + kGroupPad - 1) / kGroupPad * kGroupPad;
+    if (PASS == 1) {
+      for (; u < u_end; ++u)
+#pragma unroll
+        for (int r = 0; r < R; ++r)
+          gent[R * u + r] = make_float4(0.f, 0.f, 0.f, r == 0 ? __int_as_float((int)(R * g)) : 0.f);
+    }
+    if (PASS == 0) count[g] = u_end;
+  }
+}
+
+__global__ void k_set0(int64_t* a) { a[0] = 0; }
+
+// float2 view of V consecutive floats (V = 2 or 4)
+template <int V>
+struct F2 {
+  float2 v[V / 2];
+};
+
+template <int V>
+__device__ __forceinline__ void vld2(const float* p, F2<V>& x) {
+  if constexpr (V == 4) {
+    const float4 t = __ldg(reinterpret_cast<const float4*>(p));
+    x.v[0] = make_float2(t.x, t.y);
+    x.v[1] = make_float2(t.z, t.w);
+  } else {
+    x.v[0] = __ldg(reinterpret_cast<const float2*>(p));
+  }
+}
+
+// Narrow tile (V = 1, B = 32): one warp, one group, lane l owns column l; nc < 32
+// masks a partial last tile.
+template <int R, int B, int V, int U>
+__device__ __forceinline__ void group_rows(int64_t g, int64_t n_atoms, const int64_t* __restrict__ gptr,
+                                           const float4* __restrict__ gent, const float* __restrict__ diag,
+                                           const float* __restrict__ X, int64_t ldx, float* Y, int64_t ldy,
+                                           const float* Yin, int64_t ldyin, float* __restrict__ Acc, int64_t ldacc,
+                                           int c0, int nc, const Epi& ep, const double* __restrict__ Q,
+                                           int64_t ndof, const double* s_coef, int lane) {
+  static_assert(B == 32 && V == 1, "narrow tile");
+  // acc holds +sum_j w (w . X_j); row_out negates it
+  float acc[R][3][1][1];
+#pragma unroll
+  for (int r = 0; r < R; ++r) acc[r][0][0][0] = acc[r][1][0][0] = acc[r][2][0][0] = 0.f;
+  const int64_t u1 = gptr[g + 1];
+  const float* Xc = X + c0 + lane;
+  const bool live = lane < nc;
+#pragma unroll U
+  for (int64_t u = gptr[g]; u < u1; ++u) {
+    float4 s[R];
+#pragma unroll
+    for (int r = 0; r < R; ++r) s[r] = __ldg(gent + R * u + r);
+    const float* xj = Xc + 3 * (int64_t)__float_as_int(s[0].w) * ldx;
+    float x0 = 0.f, x1 = 0.f, x2 = 0.f;
+    if (live) {
+      x0 = __ldg(xj);
+      x1 = __ldg(xj + ldx);
+      x2 = __ldg(xj + 2 * ldx);
+    }
+#pragma unroll
+    for (int r = 0; r < R; ++r) {
+      const float dot = __fmaf_rn(s[r].z, x2, __fmaf_rn(s[r].y, x1, s[r].x * x0));
+      acc[r][0][0][0] = __fmaf_rn(s[r].x, dot, acc[r][0][0][0]);
+      acc[r][1][0][0] = __fmaf_rn(s[r].y, dot, acc[r][1][0][0]);
+      acc[r][2][0][0] = __fmaf_rn(s[r].z, dot, acc[r][2][0][0]);
+    }
+  }
+#pragma unroll
+  for (int r = 0; r < R; ++r) {
+    const int64_t i = R * g + r;
+    if (i < n_atoms)
+      row_out<float, B, V, true>(i, acc[r], nc, diag, X, ldx, Y, ldy, Yin, ldyin, Acc, ldacc, c0, ep, Q, ndof,
+                                 s_coef, lane);
+  }
+}
+
+// Wide tiles (V = 2 or 4, every column live): the group's unions are walked in
+// chunks of U (the store pads each group to whole chunks).  A chunk's U*R weight
+// slots are fetched one chunk ahead, one 16-byte slot per lane, then staged in
+// this warp's shared slots; the column indices come by shuffle and the weights by
+// broadcast shared loads, so the registers in flight hold only the X_j gathers.
+template <int R, int B, int V, int U>
+__device__ __forceinline__ void group_rows_staged(int64_t g, int64_t n_atoms, const int64_t* __restrict__ gptr,
+                                                  const float4* __restrict__ gent, const float* __restrict__ diag,
+                                                  const float* __restrict__ X, int64_t ldx, float* Y, int64_t ldy,
+                                                  const float* Yin, int64_t ldyin, float* __restrict__ Acc,
+                                                  int64_t ldacc, int c0, const Epi& ep, const double* __restrict__ Q,
+                                                  int64_t ndof, const double* s_coef, float4* s_w, int lane) {
+  static_assert(B == 32 * V && V >= 2, "one warp spans the tile");
+  constexpr int NS = U * R;
+  static_assert(NS <= 32, "one slot per lane");
+  float2 acc[R][3][V / 2];
+#pragma unroll
+  for (int r = 0; r < R; ++r)
+#pragma unroll
+    for (int p = 0; p < V / 2; ++p) acc[r][0][p] = acc[r][1][p] = acc[r][2][p] = make_float2(0.f, 0.f);
+  const int64_t u0 = gptr[g], u1 = gptr[g + 1];
+  const float* Xc = X + c0 + lane * V;
+  float4 wreg = make_float4(0.f, 0.f, 0.f, 0.f);
+  if (u0 < u1 && lane < NS) wreg = __ldg(gent + R * u0 + lane);
+#pragma unroll 1
+  for (int64_t u = u0; u < u1; u += U) {
+    int j[U];
+#pragma unroll
+    for (int k = 0; k < U; ++k) j[k] = __shfl_sync(0xffffffffu, __float_as_int(wreg.w), k * R);
+    __syncwarp();                        // the previous chunk's reads of s_w are done
+    if (lane < NS) s_w[lane] = wreg;
+    __syncwarp();
+    if (u + U < u1 && lane < NS) wreg = __ldg(gent + R * (u + U) + lane);
+    F2<V> x[U][3];
+#pragma unroll
+    for (int k = 0; k < U; ++k) {
+      const float* xj = Xc + 3 * (int64_t)j[k] * ldx;
+      vld2<V>(xj, x[k][0]);
+      vld2<V>(xj + ldx, x[k][1]);
+      vld2<V>(xj + 2 * ldx, x[k][2]);
+    }
+#pragma unroll
+    for (int k = 0; k < U; ++k) {
+#pragma unroll
+      for (int r = 0; r < R; ++r) {
+        const float4 w = s_w[k * R + r];
+        const float2 wx = make_float2(w.x, w.x), wy = make_float2(w.y, w.y), wz = make_float2(w.z, w.z);
+#pragma unroll
+        for (int p = 0; p < V / 2; ++p) {
+          float2 dot = __fmul2_rn(wx, x[k][0].v[p]);
+          dot = __ffma2_rn(wy, x[k][1].v[p], dot);
+          dot = __ffma2_rn(wz, x[k][2].v[p], dot);
+          acc[r][0][p] = __ffma2_rn(wx, dot, acc[r][0][p]);
+          acc[r][1][p] = __ffma2_rn(wy, dot, acc[r][1][p]);
+          acc[r][2][p] = __ffma2_rn(wz, dot, acc[r][2][p]);
+        }
+      }
+    }
+  }
+#pragma unroll
+  for (int r = 0; r < R; ++r) {
+    const int64_t i = R * g + r;
+    if (i < n_atoms) {
+      float a[3][1][V];
+#pragma unroll
+      for (int c = 0; c < 3; ++c)
+#pragma unroll
+        for (int p = 0; p < V / 2; ++p) {
+          a[c][0][2 * p] = acc[r][c][p].x;
+          a[c][0][2 * p + 1] = acc[r][c][p].y;
+        }
+      row_out<float, B, V, true>(i, a, B, diag, X, ldx, Y, ldy, Yin, ldyin, Acc, ldacc, c0, ep, Q, ndof, s_coef,
+                                 lane);
+    }
+  }
+}
+
+template <int R, int B, int V, int U>
+__device__ __forceinline__ void group_dispatch(int64_t g, int64_t n_atoms, const int64_t* __restrict__ gptr,
+                                               const float4* __restrict__ gent, const float* __restrict__ diag,
+                                               const float* __restrict__ X, int64_t ldx, float* Y, int64_t ldy,
+                                               const float* Yin, int64_t ldyin, float* __restrict__ Acc,
+                                               int64_t ldacc, int c0, int nc, const Epi& ep,
+                                               const double* __restrict__ Q, int64_t ndof, const double* s_coef,
+                                               float4* s_w, int lane) {
+  if constexpr (V >= 2)
+    group_rows_staged<R, B, V, (U * R <= 32 ? U : 32 / R)>(g, n_atoms, gptr, gent, diag, X, ldx, Y, ldy, Yin,
+                                                          ldyin, Acc, ldacc, c0, ep, Q, ndof, s_coef, s_w, lane);
+  else
+    group_rows<R, B, V, (U < 4 ? U : 4)>(g, n_atoms, gptr, gent, diag, X, ldx, Y, ldy, Yin, ldyin, Acc, ldacc, c0,
+                                         nc, ep, Q, ndof, s_coef, lane);
+}
+
+// Two resident blocks of 256 threads per SM: 128 registers a thread, which the
+// gathers of a 128-column chunk in flight fill.
+template <int R, int B, int V, int U, int NT>
+__global__ void __launch_bounds__(NT, 2)
+k_spmm_group(int64_t n_atoms, const int64_t* __restrict__ gptr, const float4* __restrict__ gent,
+             const float* __restrict__ diag, const float* __restrict__ X, int64_t ldx, float* Y, int64_t ldy,
+             const float* Yin, int64_t ldyin, float* __restrict__ Acc, int64_t ldacc, int c0, int nc, Epi ep,
+             const double* __restrict__ Q, int64_t ndof, const double* __restrict__ coef,
+             int* __restrict__ group_counter) {
+  __shared__ double s_coef[8 * B];
+  __shared__ float4 s_slots[NT / 32][32];
+  if (ep.r > 0) {
+    for (int t = threadIdx.x; t < ep.r * B; t += NT) s_coef[t] = coef[t];
+    __syncthreads();
+  }
+  const int lane = threadIdx.x & 31;
+  float4* s_w = s_slots[threadIdx.x >> 5];
+  const int64_t ng = (n_atoms + R - 1) / R;
+  if (group_counter == nullptr) {
+    for (int64_t g = (int64_t)blockIdx.x * (NT / 32) + (threadIdx.x >> 5); g < ng;
+         g += (int64_t)gridDim.x * (NT / 32))
+      group_dispatch<R, B, V, U>(g, n_atoms, gptr, gent, diag, X, ldx, Y, ldy, Yin, ldyin, Acc, ldacc, c0, nc, ep,
+                                 Q, ndof, s_coef, s_w, lane);
+    return;
+  }
+  // each warp takes chunks of kGroupSteps consecutive groups from the counter
+  for (;;) {
+    int base = 0;
+    if (lane == 0) base = atomicAdd(group_counter, kGroupSteps);
+    base = __shfl_sync(0xffffffffu, base, 0);
+    if (base >= ng) break;
+#pragma unroll 1
+    for (int st = 0; st < kGroupSteps; ++st) {
+      const int64_t g = (int64_t)base + st;
+      if (g < ng)
+        group_dispatch<R, B, V, U>(g, n_atoms, gptr, gent, diag, X, ldx, Y, ldy, Yin, ldyin, Acc, ldacc, c0, nc, ep,
+                                   Q, ndof, s_coef, s_w, lane);
+    }
+  }
+}
+
+// Unions in flight per warp of the row-group product (the autotuner's hook): 0
+// picks the default of the tile width.
+std::atomic<int> g_group_unroll{0};
+
+template <int R, int B, int V>
+cudaError_t launch_group_tile(int64_t n_atoms, const int64_t* gptr, const float4* gent, const float* diag,
+                              const float* X, int64_t ldx, float* Y, int64_t ldy, const float* Yin, int64_t ldyin,
+                              float* Acc, int64_t ldacc, int c0, int nc, Epi ep, const double* Q, double hot_shift,
+                              double* partial, double* coef, cudaStream_t stream, int* counter) {
+  const int64_t ndof = 3 * n_atoms;
+  if (ep.r > 0) {
+    dim3 g(kQxBlocks, ep.r);
+    k_qx_partial<float, B><<<g, kThreads, 0, stream>>>(Q, ndof, X, ldx, c0, partial, nc);
+    k_qx_final<<<(ep.r * B + kThreads / 32 - 1) / (kThreads / 32), kThreads, 0, stream>>>(partial, kQxBlocks,
+                                                                                          ep.r, B, hot_shift, coef);
+  }
+  if (counter != nullptr) {
+    const cudaError_t me = cudaMemsetAsync(counter, 0, sizeof(int), stream);
+    if (me != cudaSuccess) return me;
+  }
+  constexpr int NT = 256;
+  const int64_t ng = (n_atoms + R - 1) / R;
+  const int blocks = grid_for(ng, NT / 32, 148 * g_cols_blocks_per_sm.load());
+  const int un = g_group_unroll.load();
+#define GROUP_LAUNCH(UU)                                                                                      \
+  k_spmm_group<R, B, V, UU, NT><<<blocks, NT, 0, stream>>>(n_atoms, gptr, gent, diag, X, ldx, Y, ldy, Yin,    \
+                                                           ldyin, Acc, ldacc, c0, nc, ep, Q, ndof, coef, counter)
+  // default: 16 unions in flight on 128-column tiles, 8 on narrower ones (the
+  // fastest on the 100k-atom assembly and the 500k-atom shell)
+  if (un == 16 || (un == 0 && B == 128)) GROUP_LAUNCH(16);
+  else if (un == 4) GROUP_LAUNCH(4);
+  else if (un == 2) GROUP_LAUNCH(2);
+  else GROUP_LAUNCH(8);
+#undef GROUP_LAUNCH
+  return cudaGetLastError();
+}
+
+template <int R>
+cudaError_t run_groups(int64_t n_atoms, const int64_t* gptr, const float4* gent, const float* D, const float* X,
+                       int64_t ldx, int b, float* Y, int64_t ldy, const float* Yin, int64_t ldyin, float* Acc,
+                       int64_t ldacc, Epi ep, const double* Q, double hot_shift, double* partial, double* coef,
+                       cudaStream_t s, int* counter) {
+  auto al = [&](int m) {
+    const uintptr_t a = (uintptr_t)m * sizeof(float);
+    bool ok = (ldx % m == 0) && (ldy % m == 0) && ((uintptr_t)X % a == 0) && ((uintptr_t)Y % a == 0);
+    if (ep.has_yin) ok = ok && (ldyin % m == 0) && ((uintptr_t)Yin % a == 0);
+    if (ep.accumulate) ok = ok && (ldacc % m == 0) && ((uintptr_t)Acc % a == 0);
+    return ok;
+  };
+  const bool al4 = al(4), al2 = al(2);
+  int c0 = 0;
+  cudaError_t e = cudaSuccess;
+  while (c0 < b && e == cudaSuccess) {
+    const int rem = b - c0;
+    if (rem >= 128 && al4 && c0 % 4 == 0) {
+      e = launch_group_tile<R, 128, 4>(n_atoms, gptr, gent, D, X, ldx, Y, ldy, Yin, ldyin, Acc, ldacc, c0, 128, ep,
+                                       Q, hot_shift, partial, coef, s, counter);
+      c0 += 128;
+    } else if (rem >= 64 && al2 && c0 % 2 == 0) {
+      e = launch_group_tile<R, 64, 2>(n_atoms, gptr, gent, D, X, ldx, Y, ldy, Yin, ldyin, Acc, ldacc, c0, 64, ep, Q,
+                                      hot_shift, partial, coef, s, counter);
+      c0 += 64;
+    } else {
+      const int nc = rem < 32 ? rem : 32;
+      e = launch_group_tile<R, 32, 1>(n_atoms, gptr, gent, D, X, ldx, Y, ldy, Yin, ldyin, Acc, ldacc, c0, nc, ep, Q,
+                                      hot_shift, partial, coef, s, counter);
+      c0 += nc;
+    }
   }
   return e;
 }
@@ -832,6 +1214,167 @@ extern "C" inch_status inch_spmm_seg_ws(int32_t prec, int64_t n_atoms, const int
     err = run<double>(n_atoms, rowptr, ent, diag, X, ldx, b, Y, ldy, Yin, ldyin, nullptr, 0, ep, nullptr, 0.0,
                       nullptr, nullptr, stream, counter);
   INCH_REQUIRE(err == cudaSuccess, INCH_CUDA_ERROR, "inch_spmm_seg_ws: %s", cudaGetErrorString(err));
+  return INCH_OK;
+}
+
+// ---------------------------------------------------------------------------
+// Row-group layout: build and product.
+// ---------------------------------------------------------------------------
+extern "C" size_t inch_group_store_workspace_size(int64_t n_atoms, int32_t rows_per_group) {
+  const int R = rows_per_group > 0 ? rows_per_group : 1;
+  const int64_t ng = (n_atoms + R - 1) / R;
+  size_t cb = 0;
+  cub::DeviceScan::InclusiveSum(nullptr, cb, (int64_t*)nullptr, (int64_t*)nullptr, (int)(ng > 0 ? ng : 1));
+  Sizer s;
+  s.take<int64_t>(ng > 0 ? ng : 1);
+  s.take<char>(cb);
+  return s.bytes();
+}
+
+extern "C" inch_status inch_group_store_count(const int64_t* rowptr, const float* ent32, int64_t n_atoms,
+                                              int32_t rows_per_group, int64_t* group_ptr, int64_t* n_union_host,
+                                              void* ws, size_t ws_bytes, cudaStream_t stream) {
+  INCH_REQUIRE(rowptr && ent32 && group_ptr && n_union_host, INCH_INVALID_ARG,
+               "inch_group_store_count: NULL argument");
+  INCH_REQUIRE(rows_per_group == 2 || rows_per_group == 4, INCH_INVALID_ARG,
+               "inch_group_store_count: rows_per_group must be 2 or 4");
+  INCH_REQUIRE(n_atoms >= 1 && n_atoms < (int64_t(1) << 31), INCH_INVALID_ARG,
+               "inch_group_store_count: n_atoms out of range");
+  INCH_REQUIRE(((uintptr_t)ent32 & 15) == 0, INCH_INVALID_ARG,
+               "inch_group_store_count: entries must be 16-byte aligned");
+  const int R = rows_per_group;
+  const int64_t ng = (n_atoms + R - 1) / R;
+  Carver c(ws, ws_bytes);
+  int64_t* cnt = c.take<int64_t>(ng);
+  size_t cb = 0;
+  cub::DeviceScan::InclusiveSum(nullptr, cb, (int64_t*)nullptr, (int64_t*)nullptr, (int)ng);
+  void* tmp = c.take<char>(cb);
+  INCH_REQUIRE(c.ok, INCH_OOM, "inch_group_store_count: workspace of %zu bytes, need %zu", ws_bytes,
+               inch_group_store_workspace_size(n_atoms, R));
+  const int blocks = grid_for(ng, kGroupBuildThreads, 148 * 16);
+  const float4* e4 = reinterpret_cast<const float4*>(ent32);
+  if (R == 2)
+    k_group_merge<0, 2><<<blocks, kGroupBuildThreads, 0, stream>>>(n_atoms, rowptr, e4, cnt, nullptr, nullptr);
+  else
+    k_group_merge<0, 4><<<blocks, kGroupBuildThreads, 0, stream>>>(n_atoms, rowptr, e4, cnt, nullptr, nullptr);
+  INCH_LAUNCH_CHECK();
+  k_set0<<<1, 1, 0, stream>>>(group_ptr);
+  INCH_LAUNCH_CHECK();
+  INCH_CUDA(cub::DeviceScan::InclusiveSum(tmp, cb, cnt, group_ptr + 1, (int)ng, stream));
+  INCH_CUDA(cudaMemcpyAsync(n_union_host, group_ptr + ng, sizeof(int64_t), cudaMemcpyDeviceToHost, stream));
+  INCH_CUDA(cudaStreamSynchronize(stream));
+  return INCH_OK;
+}
+
+extern "C" inch_status inch_group_store_fill(const int64_t* rowptr, const float* ent32, int64_t n_atoms,
+                                             int32_t rows_per_group, const int64_t* group_ptr, float* group_ent,
+                                             cudaStream_t stream) {
+  INCH_REQUIRE(rowptr && ent32 && group_ptr && group_ent, INCH_INVALID_ARG, "inch_group_store_fill: NULL argument");
+  INCH_REQUIRE(rows_per_group == 2 || rows_per_group == 4, INCH_INVALID_ARG,
+               "inch_group_store_fill: rows_per_group must be 2 or 4");
+  INCH_REQUIRE(n_atoms >= 1 && n_atoms < (int64_t(1) << 31), INCH_INVALID_ARG,
+               "inch_group_store_fill: n_atoms out of range");
+  INCH_REQUIRE(((uintptr_t)ent32 & 15) == 0 && ((uintptr_t)group_ent & 15) == 0, INCH_INVALID_ARG,
+               "inch_group_store_fill: entry buffers must be 16-byte aligned");
+  const int R = rows_per_group;
+  const int64_t ng = (n_atoms + R - 1) / R;
+  const int blocks = grid_for(ng, kGroupBuildThreads, 148 * 16);
+  const float4* e4 = reinterpret_cast<const float4*>(ent32);
+  float4* g4 = reinterpret_cast<float4*>(group_ent);
+  if (R == 2)
+    k_group_merge<1, 2><<<blocks, kGroupBuildThreads, 0, stream>>>(n_atoms, rowptr, e4, nullptr, group_ptr, g4);
+  else
+    k_group_merge<1, 4><<<blocks, kGroupBuildThreads, 0, stream>>>(n_atoms, rowptr, e4, nullptr, group_ptr, g4);
+  INCH_LAUNCH_CHECK();
+  return INCH_OK;
+}
+
+extern "C" inch_status inch_spmm_group_tune(int32_t unroll) {
+  INCH_REQUIRE(unroll == 0 || unroll == 2 || unroll == 4 || unroll == 8 || unroll == 16, INCH_INVALID_ARG,
+               "inch_spmm_group_tune: unroll must be 0, 2, 4, 8 or 16");
+  g_group_unroll.store(unroll);
+  return INCH_OK;
+}
+
+namespace {
+inch_status groups_common(const char* who, int64_t n_atoms, int32_t R, const int64_t* gptr, const float* gent,
+                          const float* diag, const float* X, int64_t ldx, int32_t b, float* Y, int64_t ldy) {
+  INCH_REQUIRE(gptr && gent && diag && X && Y, INCH_INVALID_ARG, "%s: NULL argument", who);
+  INCH_REQUIRE(R == 2 || R == 4, INCH_INVALID_ARG, "%s: rows_per_group must be 2 or 4", who);
+  INCH_REQUIRE(n_atoms >= 1 && n_atoms < (int64_t(1) << 31), INCH_INVALID_ARG, "%s: n_atoms out of range", who);
+  INCH_REQUIRE(b >= 1 && ldx >= b && ldy >= b, INCH_INVALID_ARG, "%s: b=%d or leading dimension below b", who, b);
+  INCH_REQUIRE((const void*)X != (const void*)Y, INCH_INVALID_ARG, "%s: X and Y must not alias", who);
+  INCH_REQUIRE(((uintptr_t)gent & 15) == 0 && ((uintptr_t)diag & 15) == 0, INCH_INVALID_ARG,
+               "%s: store buffers must be 16-byte aligned", who);
+  return INCH_OK;
+}
+}  // namespace
+
+extern "C" inch_status inch_spmm_groups(int64_t n_atoms, int32_t rows_per_group, const int64_t* group_ptr,
+                                        const float* group_ent, const float* diag, const float* X, int64_t ldx,
+                                        int32_t b, float* Y, int64_t ldy, const float* Yin, int64_t ldyin, float* Acc,
+                                        int64_t ldacc, const double* q, const inch_spmm_epilogue* ep_in, void* ws,
+                                        size_t ws_bytes, cudaStream_t stream) {
+  const inch_status st = groups_common("inch_spmm_groups", n_atoms, rows_per_group, group_ptr, group_ent, diag, X,
+                                       ldx, b, Y, ldy);
+  if (st != INCH_OK) return st;
+  INCH_REQUIRE(ep_in != nullptr, INCH_INVALID_ARG, "inch_spmm_groups: NULL epilogue");
+  const inch_spmm_epilogue& e = *ep_in;
+  INCH_REQUIRE(e.r >= 0 && e.r <= 8, INCH_INVALID_ARG, "inch_spmm_groups: deflation rank %d outside 0..8", e.r);
+  INCH_REQUIRE(e.r == 0 || q != nullptr, INCH_INVALID_ARG, "inch_spmm_groups: deflation basis is NULL");
+  INCH_REQUIRE(e.beta == 0.0 || (Yin != nullptr && ldyin >= b), INCH_INVALID_ARG,
+               "inch_spmm_groups: beta != 0 needs Yin");
+  INCH_REQUIRE(!e.accumulate || (Acc != nullptr && ldacc >= b), INCH_INVALID_ARG,
+               "inch_spmm_groups: accumulate needs Acc");
+  double *partial = nullptr, *coef = nullptr;
+  int* counter = nullptr;
+  if (ws != nullptr || e.r > 0) {
+    Carver c(ws, ws_bytes);
+    counter = c.take<int>(1);
+    partial = c.take<double>((size_t)kQxBlocks * 8 * 128);
+    coef = c.take<double>(8 * 128);
+    INCH_REQUIRE(c.ok, INCH_OOM, "inch_spmm_groups: workspace of %zu bytes, need %zu", ws_bytes,
+                 inch_spmm_workspace_size(n_atoms, b, e.r));
+  }
+  Epi ep{e.alpha, e.gamma, e.beta, e.mu, e.r, e.accumulate, (e.beta != 0.0) ? 1 : 0};
+  const float4* g4 = reinterpret_cast<const float4*>(group_ent);
+  const cudaError_t err =
+      rows_per_group == 2
+          ? run_groups<2>(n_atoms, group_ptr, g4, diag, X, ldx, b, Y, ldy, Yin, ldyin, Acc, ldacc, ep, q, e.hot_shift,
+                          partial, coef, stream, counter)
+          : run_groups<4>(n_atoms, group_ptr, g4, diag, X, ldx, b, Y, ldy, Yin, ldyin, Acc, ldacc, ep, q, e.hot_shift,
+                          partial, coef, stream, counter);
+  INCH_REQUIRE(err == cudaSuccess, INCH_CUDA_ERROR, "inch_spmm_groups: %s", cudaGetErrorString(err));
+  return INCH_OK;
+}
+
+extern "C" inch_status inch_spmm_groups_seg(int64_t n_atoms, int32_t rows_per_group, const int64_t* group_ptr,
+                                            const float* group_ent, const float* diag, const float* X, int64_t ldx,
+                                            int32_t b, float* Y, int64_t ldy, const float* Yin, int64_t ldyin,
+                                            const int32_t* atom_seg, const double* seg_coef, void* ws,
+                                            size_t ws_bytes, cudaStream_t stream) {
+  const inch_status st = groups_common("inch_spmm_groups_seg", n_atoms, rows_per_group, group_ptr, group_ent, diag,
+                                       X, ldx, b, Y, ldy);
+  if (st != INCH_OK) return st;
+  INCH_REQUIRE(atom_seg && seg_coef, INCH_INVALID_ARG, "inch_spmm_groups_seg: NULL segment arrays");
+  INCH_REQUIRE(Yin == nullptr || ldyin >= b, INCH_INVALID_ARG, "inch_spmm_groups_seg: ldyin below b");
+  int* counter = nullptr;
+  if (ws != nullptr) {
+    Carver c(ws, ws_bytes);
+    counter = c.take<int>(1);
+    INCH_REQUIRE(c.ok, INCH_OOM, "inch_spmm_groups_seg: workspace too small");
+  }
+  Epi ep{0.0, 0.0, 0.0, 0.0, 0, 0, Yin != nullptr ? 1 : 0};
+  ep.seg_coef = seg_coef;
+  ep.atom_seg = atom_seg;
+  const float4* g4 = reinterpret_cast<const float4*>(group_ent);
+  const cudaError_t err =
+      rows_per_group == 2
+          ? run_groups<2>(n_atoms, group_ptr, g4, diag, X, ldx, b, Y, ldy, Yin, ldyin, nullptr, 0, ep, nullptr, 0.0,
+                          nullptr, nullptr, stream, counter)
+          : run_groups<4>(n_atoms, group_ptr, g4, diag, X, ldx, b, Y, ldy, Yin, ldyin, nullptr, 0, ep, nullptr, 0.0,
+                          nullptr, nullptr, stream, counter);
+  INCH_REQUIRE(err == cudaSuccess, INCH_CUDA_ERROR, "inch_spmm_groups_seg: %s", cudaGetErrorString(err));
   return INCH_OK;
 }
 

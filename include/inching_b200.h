@@ -416,6 +416,48 @@ inch_status inch_spmm_band_tune(int32_t widest_fp32_panel);
  * No reference counterpart. */
 inch_status inch_spmm_band_status(int32_t* status_host);
 
+/* ---------------------------------------------------------------------------
+ * Row-group store, FP32 (no reference counterpart; an alternative layout of the
+ * same matrix, built from the FP32 pair entries of inch_hessian_assemble).
+ * R = rows_per_group (2 or 4) consecutive atoms form a group; the group's
+ * neighbour lists are merged into one sorted union, and union u stores R float4
+ * slots group_ent[R*u + r] = {wx, wy, wz, .} of row R*g + r's entry for that
+ * column (zeros where the row has none), slot 0's last field holding the column
+ * index as int bits.  Each group's union count is padded with zero-weight unions
+ * to a multiple of 16.  group_ptr: (ceil(n_atoms / R) + 1) offsets in unions.
+ * A row's entries keep their order, so the product gives the bits of inch_spmm
+ * on the pair store.  count (synchronises, returns the union total) then fill
+ * (group_ent: n_union * R float4, 16-byte aligned). */
+size_t inch_group_store_workspace_size(int64_t n_atoms, int32_t rows_per_group);
+inch_status inch_group_store_count(const int64_t* rowptr_dev, const float* ent32_dev, int64_t n_atoms,
+                                   int32_t rows_per_group, int64_t* group_ptr_dev, int64_t* n_union_host,
+                                   void* ws_dev, size_t ws_bytes, cudaStream_t stream);
+inch_status inch_group_store_fill(const int64_t* rowptr_dev, const float* ent32_dev, int64_t n_atoms,
+                                  int32_t rows_per_group, const int64_t* group_ptr_dev, float* group_ent_dev,
+                                  cudaStream_t stream);
+/* The row-group product: inch_spmm (prec 32) on the row-group store, any b >= 1
+ * (tiles of 128 / 64 columns where the vector blocks allow float4 / float2
+ * access, else 32-column tiles, the last one partial).  One warp per group and
+ * tile; each X_j gather serves every row of the group.  Replaces the same two
+ * cuSPARSE SpMVs as inch_spmm (Burn/Krylov/T3.py:138-156), with the same fused
+ * epilogue.  ws: inch_spmm_workspace_size() bytes (row counter and deflation
+ * scratch), or NULL when ep->r == 0. */
+inch_status inch_spmm_groups(int64_t n_atoms, int32_t rows_per_group, const int64_t* group_ptr_dev,
+                             const float* group_ent_dev, const float* diag_dev, const float* X_dev, int64_t ldx,
+                             int32_t b, float* Y_dev, int64_t ldy, const float* Yin_dev, int64_t ldyin,
+                             float* Acc_dev, int64_t ldacc, const double* q_dev, const inch_spmm_epilogue* ep,
+                             void* ws_dev, size_t ws_bytes, cudaStream_t stream);
+/* inch_spmm_seg on the row-group store (per-segment alpha, gamma, beta; any b). */
+inch_status inch_spmm_groups_seg(int64_t n_atoms, int32_t rows_per_group, const int64_t* group_ptr_dev,
+                                 const float* group_ent_dev, const float* diag_dev, const float* X_dev, int64_t ldx,
+                                 int32_t b, float* Y_dev, int64_t ldy, const float* Yin_dev, int64_t ldyin,
+                                 const int32_t* atom_seg_dev, const double* seg_coef_dev, void* ws_dev,
+                                 size_t ws_bytes, cudaStream_t stream);
+/* Unions a warp of the row-group product keeps in flight (2, 4, 8 or 16; 0 = the
+ * default: 16 on 128-column tiles, 8 on narrower ones): the autotuner's hook (no
+ * reference counterpart). */
+inch_status inch_spmm_group_tune(int32_t unroll);
+
 /* Allocation-free form of inch_spmm (no counterpart in the reference).  For
  * callers that cannot provide device scratch -- hosts running on another
  * runtime's memory manager without a device allocator of their own, or thin FFI

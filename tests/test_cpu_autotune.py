@@ -8,16 +8,18 @@ import torch
 
 COST = {("pairs", 256, 5, 1): 3.0, ("pairs", 256, 5, 0): 2.2, ("pairs", 256, 5, 2): 2.9,
         ("pairs", 256, 4, 1): 2.0, ("pairs", 512, 2, 1): 2.5, ("pairs", 0, 4, 0): 1.5,
-        ("tiles", 256, 5, 1): 1.0}
+        ("groups", 256, 5, 1): 1.2, ("tiles", 256, 5, 1): 1.0}
 
 
 class FakeStore:
-    def __init__(self, tiles):
+    def __init__(self, tiles, groups=False):
         self.n_atoms, self.nnz_blocks = 100, 900
         self.shape = (300, 300)
         self.device = torch.device("cpu")
         self.tiles = {} if tiles else None
         self.use_tiles = False
+        self.groups = {} if groups else None
+        self.use_groups = False
         self.keep_pairs = True
         self.spmm_cfg = {}
         self.calls = 0
@@ -37,7 +39,12 @@ def test_autotuner_picks_fastest_and_caches(monkeypatch):
 
     def timer(fn, reps):
         fn()
-        cfg = ("tiles", 256, 5, 1) if H.use_tiles else (("pairs",) + applied[-1])
+        if H.use_tiles:
+            cfg = ("tiles", 256, 5, 1)
+        elif H.use_groups:
+            cfg = ("groups",) + applied[-1]
+        else:
+            cfg = ("pairs",) + applied[-1]
         timed.append(cfg)
         return COST[cfg]
 
@@ -55,6 +62,19 @@ def test_autotuner_picks_fastest_and_caches(monkeypatch):
     best, table = autotune.tune_spmm(H, 64, timer=timer)
     assert best == ("tiles", 256, 5, 1) and H.use_tiles and len(table) == 7
     assert H.spmm_cfg[(32, 64)] == best
+    # the row-group layout: timed for FP32 products of >= 64 columns when built
+    H = FakeStore(tiles=False, groups=True)
+    H.nnz_blocks = 902
+    best, table = autotune.tune_spmm(H, 128, timer=timer)
+    assert best == ("groups", 256, 5, 1) and H.use_groups and not H.use_tiles and len(table) == 7
+    autotune.apply_config(H, ("pairs", 256, 5, 1))
+    assert not H.use_groups
+    H.nnz_blocks = 903
+    best, table = autotune.tune_spmm(H, 32, timer=timer)     # narrower than one group tile
+    assert ("groups", 256, 5, 1) not in table and best == ("pairs", 0, 4, 0)
+    H.nnz_blocks = 904
+    best, table = autotune.tune_spmm(H, 64, prec=64, timer=timer)   # FP64: pair layout only
+    assert ("groups", 256, 5, 1) not in table
     autotune._cache.clear()
 
 
@@ -69,6 +89,10 @@ def test_launch_hooks_accept_documented_settings_only():
         _native.spmm_tune(256, 5, 3)
     _native.spmm_band_tune(64)
     _native.spmm_band_tune(128)
+    for u in (0, 2, 4, 8, 16):
+        _native.spmm_group_tune(u)
+    with pytest.raises(AssertionError):
+        _native.spmm_group_tune(3)
     with pytest.raises(AssertionError):
         _native.spmm_band_tune(96)
     autotune.reset()
