@@ -4,7 +4,9 @@ neighbour lists, FP32) against the pair-layout kernel and the FP64 oracle
 PolynomialFilters/T2.py:59-80).
 
 Each row of a group sums its own entries in the pair layout's order (zero-weight
-slots in between add exact zeros), so without deflation the group product is
+slots in between add exact zeros), the order of the pair layout's wide kernel
+(tiles of >= 8 columns; its narrower tiles split a row's entries over lanes).  So
+without deflation, at widths that are multiples of 8, the group product is
 compared with the pair kernel for bit equality, over every tile width (128 / 64
 float4 / float2 tiles, 32-column tiles, partial last tiles), every in-flight
 setting, unaligned blocks, the per-segment epilogue, periodic images (repeated
@@ -52,6 +54,14 @@ def _pair(H, X, Y=None, **kw):
         k = {key: (v[:, sl] if key in ("Yin", "acc") and v is not None else v) for key, v in kw.items()}
         _native.spmm(32, H.n_atoms, H.rowptr, ent, diag, X[:, sl], Y[:, sl], **k)
     return Y
+
+
+def _same(Yg, Yp):
+    """Bit equality where the pair kernel ran only wide tiles (b % 8 == 0), else
+    agreement within FP32 rounding of the differently ordered sums."""
+    if Yg.shape[-1] % 8 == 0:
+        return torch.equal(Yg, Yp)
+    return float((Yg - Yp).abs().max()) <= 1e-5 * (float(Yp.abs().max()) + 1.0)
 
 
 def _merge_reference(rowptr, cols, ent, n, R, pad=16):
@@ -103,7 +113,7 @@ def test_group_store_layout_matches_host_merge(case, R):
 
 @pytest.mark.parametrize("b", [1, 5, 31, 32, 33, 64, 96, 100, 128, 129, 200, 320])
 @pytest.mark.parametrize("R", [2, 4])
-def test_group_product_bit_equal_to_pair_kernel(case, R, b):
+def test_group_product_matches_pair_kernel(case, R, b):
     from inching_b200 import _native
     Xr, H, A, Ad, scale = case
     gptr, gent, nu = _stores(H)[R]
@@ -113,7 +123,7 @@ def test_group_product_bit_equal_to_pair_kernel(case, R, b):
     X = torch.randn((H.shape[0], b), generator=g, dtype=torch.float32, device="cuda")
     Yg = torch.full_like(X, float("nan"))
     _native.spmm_groups(H.n_atoms, R, gptr, gent, diag, X, Yg)
-    assert torch.equal(Yg, _pair(H, X))
+    assert _same(Yg, _pair(H, X))
 
 
 @pytest.mark.parametrize("unroll", [0, 2, 4, 8, 16])
@@ -188,13 +198,14 @@ def test_group_fused_epilogue(case, R, b):
 
 def test_group_unaligned_blocks_and_untouched_columns(case):
     """Odd leading dimension and column offset: the group product runs 32-column
-    tiles (no vector access), gives the pair kernel's bits, and leaves the columns
+    tiles (no vector access, the last one partial), gives the pair kernel's bits,
+    and leaves the columns
     outside the view untouched."""
     from inching_b200 import _native
     Xr, H, A, Ad, scale = case
     gptr, gent, nu = _stores(H)[2]
     _, diag = H.store(32)
-    b, ld = 70, 73
+    b, ld = 72, 73
     g = torch.Generator(device="cuda")
     g.manual_seed(11)
     Xt = torch.randn((H.shape[0], ld), generator=g, dtype=torch.float32, device="cuda")
@@ -236,7 +247,7 @@ def test_group_segmented_matches_pair_kernel(case, R):
 @pytest.mark.parametrize("n", [1, 2, 3, 5, 9])
 def test_group_tiny_stores(n):
     """Stores smaller than a group or with a partial last group, an isolated atom
-    and a coincident pair: every tile width gives the pair kernel's bits."""
+    and a coincident pair: every tile width gives the pair kernel's product."""
     from inching_b200 import _native
     from inching_b200.hessian import HessianStore
     rng = np.random.default_rng(n)
@@ -252,7 +263,7 @@ def test_group_tiny_stores(n):
             Xv = torch.from_numpy(rng.standard_normal((3 * n, b))).float().cuda().contiguous()
             Yg = torch.empty_like(Xv)
             _native.spmm_groups(n, R, gptr, gent, diag, Xv, Yg)
-            assert torch.equal(Yg, _pair(H, Xv)), (R, b)
+            assert _same(Yg, _pair(H, Xv)), (R, b)
 
 
 def test_group_periodic_and_weighted_stores():
