@@ -205,7 +205,7 @@ def test_group_unaligned_blocks_and_untouched_columns(case):
     Xr, H, A, Ad, scale = case
     gptr, gent, nu = _stores(H)[2]
     _, diag = H.store(32)
-    b, ld = 72, 73
+    b, ld = 72, 75
     g = torch.Generator(device="cuda")
     g.manual_seed(11)
     Xt = torch.randn((H.shape[0], ld), generator=g, dtype=torch.float32, device="cuda")
