@@ -37,11 +37,11 @@ sys.path.insert(0, ROOT)
 METRIC = "time-to-k-modes (s) at resid <=1e-6||H||"
 # From the ncu capture of the 128-column FP32 pair-kernel launch on the 100k-atom
 # assembly (the file under profiles/ named below holds the command and the figures).
-TRAFFIC_B128_BYTES = 456_450_304
-TRAFFIC_B128_RATIO = 0.966
-TRAFFIC_SOURCE = "profiles/spmm_f32_b128_assembly100k.md"
-LIMITER_FRAC = 0.771
-LIMITER_SOURCE = "profiles/spmm_f32_b128_assembly100k.md"
+TRAFFIC_B128_BYTES = 566_750_464
+TRAFFIC_B128_RATIO = 1.200
+TRAFFIC_SOURCE = "profiles/spmm_group_f32_b128_assembly100k.md"
+LIMITER_FRAC = 0.868
+LIMITER_SOURCE = "profiles/spmm_group_f32_b128_assembly100k.md"
 UNIT = "s"
 
 
@@ -183,6 +183,18 @@ def peaks():
         return float(d["hbm_gbs"]), "measured"
     except (OSError, KeyError, ValueError):
         return 6650.0, "fallback"
+
+
+def _autotune_choices(n_atoms):
+    """The autotuner's launch choice and candidate times (ms, fastest of its runs) for
+    the store of n_atoms atoms, per (precision, width class)."""
+    from inching_b200 import autotune
+    out = {}
+    for (n, nnz, wc, prec, dev), (best, table) in autotune._cache.items():
+        if n == n_atoms:
+            out[f"f{prec}_b{wc}"] = {"chosen": "/".join(str(x) for x in best),
+                                     "ms": {"/".join(str(x) for x in c): round(t, 4) for c, t in table.items()}}
+    return out
 
 
 def run_ours(args):
@@ -371,22 +383,24 @@ def run_ours(args):
                                          "d2h_bytes_per_step": int(d2h)},
         "roofline": {"bound": "hbm", "achieved": round(achieved, 1) if achieved else None, "peak": hbm,
                      "unit": "GB/s", "frac": round(achieved / hbm, 4) if achieved else None,
-                     "peak_kind": peak_kind, "kernel": "FP32 SpMM (k_spmm_cols<float, 128, 4> / k_spmm)",
+                     "peak_kind": peak_kind, "kernel": "FP32 SpMM on the row-group layout (k_spmm_group<2, 128, 4, 16>; pair kernels for "
+                               "narrow products)",
                      "spmm_calls": sp["calls"], "spmm_ms": round(sp["ms"], 2),
-                     # ncu dram__bytes_read.sum + dram__bytes_write.sum of one 64-column FP32 launch on this
+                     # ncu dram__bytes_read.sum + dram__bytes_write.sum of one 128-column FP32 launch on this
                      # workload: not measured by this run, copied from the profile named in traffic_source
                      "traffic": TRAFFIC_B128_BYTES, "traffic_unit": "bytes per 128-column launch",
                      "traffic_over_algorithmic": TRAFFIC_B128_RATIO, "traffic_source": TRAFFIC_SOURCE,
                      "traffic_measured_in_this_run": False,
                      # what bounds the kernel instead of HBM, from an ncu memory capture of the same
                      # launch; not measured by this run
-                     "limiter": {"unit": "L2 throughput (X_j gathers miss L1: 6.8 % hit rate)",
+                     "limiter": {"unit": "L1TEX throughput (X_j gathers through L1, 11.9 % hit rate; L2 at 72 %)",
                                  "throughput_frac": LIMITER_FRAC,
                                  "source": LIMITER_SOURCE, "measured_in_this_run": False}},
         "cpu_baseline": cpu,
         "clocks": clk.summary(),
         "gpu_launches": int(launches),
         "solver_info": {kk: info[kk] for kk in ("iterations", "n_spmm_filter", "n_rr", "block", "degree")},
+        "autotune": _autotune_choices(info["n_atoms"]),
         "largest_config": largest,
     }
     print(json.dumps(line))

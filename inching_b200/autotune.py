@@ -34,17 +34,19 @@ def _width_class(b):
     return width_class(b)
 
 
-def _apply(H, cfg):
-    apply_config(H, cfg)
+def _apply(H, cfg, prec=32):
+    apply_config(H, cfg, prec)
 
 
-def apply_config(H, cfg):
-    """Make cfg = (layout, threads, blocks per SM, traversal) the current choice."""
+def apply_config(H, cfg, prec=32):
+    """Make cfg = (layout, threads, blocks per SM, traversal) the current choice for
+    products at precision prec.  The row-group layout holds FP32 entries only, so
+    only an FP32 choice switches it on or off."""
     layout, threads, bps, trav = cfg
     if layout in ("pairs", "groups"):
         _native.spmm_tune(threads, bps, trav)
     H.use_tiles = layout == "tiles"
-    if getattr(H, "groups", None) is not None:
+    if getattr(H, "groups", None) is not None and prec == 32:
         H.use_groups = layout == "groups"
 
 
@@ -66,12 +68,12 @@ def _device_name(dev):
     return torch.cuda.get_device_name(dev) if dev.type == "cuda" else dev.type
 
 
-def tune_spmm(H, b, prec=32, reps=3, candidates=CANDIDATES, timer=cuda_event_ms):
+def tune_spmm(H, b, prec=32, reps=5, candidates=CANDIDATES, timer=cuda_event_ms):
     """Pick and apply the fastest configuration for (H, b, prec); returns (cfg, ms
     table).  timer(fn, reps) -> ms measures one candidate."""
     key = (H.n_atoms, H.nnz_blocks, _width_class(b), prec, _device_name(H.device))
     if key in _cache:
-        _apply(H, _cache[key][0])
+        _apply(H, _cache[key][0], prec)
         _remember(H, prec, b, _cache[key][0])
         return _cache[key]
     dt = torch.float64 if prec == 64 else torch.float32
@@ -86,10 +88,10 @@ def tune_spmm(H, b, prec=32, reps=3, candidates=CANDIDATES, timer=cuda_event_ms)
             continue
         if cfg[0] == "pairs" and not H.keep_pairs:
             continue
-        _apply(H, cfg)
+        _apply(H, cfg, prec)
         table[cfg] = timer(lambda: H.matmul(X, out=Y, prec=prec), reps)
     best = min(table, key=table.get)
-    _apply(H, best)
+    _apply(H, best, prec)
     _remember(H, prec, b, best)
     _cache[key] = (best, table)
     return best, table

@@ -175,7 +175,7 @@ class HessianStore:
             cfg = self.spmm_cfg.get((prec, width_class(1 if X.dim() == 1 else X.shape[1])))
             if cfg is not None:
                 from .autotune import apply_config
-                apply_config(self, cfg)
+                apply_config(self, cfg, prec)
         ent, diag = self.store(prec)
         probe = _probe if (_probe is not None and (_probe.prec is None or _probe.prec == prec)) else None
         if probe is not None:

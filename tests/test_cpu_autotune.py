@@ -26,6 +26,7 @@ class FakeStore:
 
     def matmul(self, X, out=None, prec=32):
         self.calls += 1
+        self.last_prec = prec
         out.copy_(X)
         return out
 
@@ -41,7 +42,7 @@ def test_autotuner_picks_fastest_and_caches(monkeypatch):
         fn()
         if H.use_tiles:
             cfg = ("tiles", 256, 5, 1)
-        elif H.use_groups:
+        elif H.use_groups and H.last_prec == 32:      # the row groups hold FP32 entries only
             cfg = ("groups",) + applied[-1]
         else:
             cfg = ("pairs",) + applied[-1]
@@ -73,8 +74,10 @@ def test_autotuner_picks_fastest_and_caches(monkeypatch):
     best, table = autotune.tune_spmm(H, 32, timer=timer)     # narrower than one group tile
     assert ("groups", 256, 5, 1) not in table and best == ("pairs", 0, 4, 0)
     H.nnz_blocks = 904
+    H.use_groups = True
     best, table = autotune.tune_spmm(H, 64, prec=64, timer=timer)   # FP64: pair layout only
     assert ("groups", 256, 5, 1) not in table
+    assert H.use_groups                     # an FP64 choice leaves the FP32 layout alone
     autotune._cache.clear()
 
 
