@@ -15,9 +15,14 @@ choice before each product, so stores of different sizes keep their own):
     the X_j rows in L2 on large structures);
   * the whole-warp-row kernel with batched gathers ("pairs", 0, ...).
 Results are cached per (atoms, pairs, width class, precision, device name).
-The solvers call tune_spmm once per store for the widths they use.
+The solvers call tune_spmm once per store for the widths they use.  The
+environment variable INCH_SPMM_LAYOUT (pairs, groups or tiles) restricts the
+candidates to one layout where the store has it (to pin the layout of a run, e.g.
+for a profile whose own timing would distort the comparison).
 """
 from __future__ import annotations
+
+import os
 
 import torch
 
@@ -78,15 +83,15 @@ def tune_spmm(H, b, prec=32, reps=5, candidates=CANDIDATES, timer=cuda_event_ms)
         return _cache[key]
     dt = torch.float64 if prec == 64 else torch.float32
     w = _width_class(b) if b >= 8 else b
+    forced = os.environ.get("INCH_SPMM_LAYOUT")
+    if forced:
+        pinned = tuple(c for c in candidates if c[0] == forced and _available(H, c, prec, w))
+        candidates = pinned or candidates
     X = torch.randn((H.shape[0], w), dtype=dt, device=H.device)
     Y = torch.empty_like(X)
     table = {}
     for cfg in candidates:
-        if cfg[0] == "tiles" and H.tiles is None:
-            continue
-        if cfg[0] == "groups" and (getattr(H, "groups", None) is None or prec != 32 or w < 64):
-            continue
-        if cfg[0] == "pairs" and not H.keep_pairs:
+        if not _available(H, cfg, prec, w):
             continue
         _apply(H, cfg, prec)
         table[cfg] = timer(lambda: H.matmul(X, out=Y, prec=prec), reps)
@@ -95,6 +100,15 @@ def tune_spmm(H, b, prec=32, reps=5, candidates=CANDIDATES, timer=cuda_event_ms)
     _remember(H, prec, b, best)
     _cache[key] = (best, table)
     return best, table
+
+
+def _available(H, cfg, prec, w):
+    """Whether the store can run candidate cfg for a w-column product at prec."""
+    if cfg[0] == "tiles":
+        return H.tiles is not None
+    if cfg[0] == "groups":
+        return getattr(H, "groups", None) is not None and prec == 32 and w >= 64
+    return H.keep_pairs
 
 
 def _remember(H, prec, b, cfg):

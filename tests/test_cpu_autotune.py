@@ -81,6 +81,27 @@ def test_autotuner_picks_fastest_and_caches(monkeypatch):
     autotune._cache.clear()
 
 
+def test_layout_pinned_by_environment(monkeypatch):
+    """INCH_SPMM_LAYOUT restricts the candidates to one layout where the store has
+    it, and is ignored where it has not."""
+    from inching_b200 import autotune
+    monkeypatch.setattr(autotune._native, "spmm_tune", lambda t, b, tr=None: None)
+    autotune._cache.clear()
+    monkeypatch.setenv("INCH_SPMM_LAYOUT", "pairs")
+    H = FakeStore(tiles=False, groups=True)
+    best, table = autotune.tune_spmm(H, 128, timer=lambda fn, reps: (fn(), 1.0)[1])
+    assert {c[0] for c in table} == {"pairs"} and not H.use_groups
+    monkeypatch.setenv("INCH_SPMM_LAYOUT", "groups")
+    H = FakeStore(tiles=False, groups=True)
+    H.nnz_blocks = 905
+    best, table = autotune.tune_spmm(H, 128, timer=lambda fn, reps: (fn(), 1.0)[1])
+    assert best[0] == "groups" and len(table) == 1 and H.use_groups
+    H.nnz_blocks = 906
+    best, table = autotune.tune_spmm(H, 64, prec=64, timer=lambda fn, reps: (fn(), 1.0)[1])
+    assert {c[0] for c in table} == {"pairs"}          # no FP64 groups: the pin is ignored
+    autotune._cache.clear()
+
+
 def test_launch_hooks_accept_documented_settings_only():
     from inching_b200 import _native, autotune
     for t, b in ((256, 5), (512, 2), (1024, 1), (0, 4)):
